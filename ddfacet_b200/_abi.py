@@ -1,0 +1,132 @@
+"""ctypes binding of libddfg.so (include/ddfg.h).
+
+The structures below mirror the C header field for field.  ``lib()`` loads the in-tree library
+(building it first if it is missing and nvcc is available) and raises if it cannot: there is no
+fallback implementation behind this module.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import threading
+
+from . import build as _build
+
+DDFG_OK = 0
+DDFG_EINVAL = -1
+DDFG_EUNSUPPORTED = -2
+DDFG_ECUDA = -3
+DDFG_EMAP = -4
+DDFG_ESIZE = -5
+DDFG_MAX_FACETS = 1024
+DDFG_FACETS_PER_LAUNCH = 16
+
+_i32 = C.c_int32
+_i64 = C.c_int64
+_f64 = C.c_double
+_vp = C.c_void_p
+
+
+class Facet(C.Structure):
+    _fields_ = [
+        ("grid", _vp),
+        ("nband", _i32), ("npol", _i32), ("ny", _i32), ("nx", _i32),
+        ("incr_x", _f64), ("incr_y", _f64),
+        ("cu", _f64), ("cv", _f64), ("l0", _f64), ("m0", _f64),
+        ("cf_data", _vp), ("cf_offset", _vp), ("cf_support", _vp),
+        ("nw", _i32), ("overs", _i32),
+        ("ref_wave", _f64), ("wmax", _f64),
+        ("idir_kms", _i32), ("idir_beam", _i32),
+        ("decorr_l", _f64), ("decorr_m", _f64),
+        ("sumwt", _vp), ("sumjones", _vp), ("sumjones_chan", _vp),
+    ]
+
+
+class VisSet(C.Structure):
+    _fields_ = [
+        ("vis", _vp), ("uvw", _vp), ("flags", _vp), ("weights", _vp), ("freqs", _vp),
+        ("freq_mean", _f64),
+        ("chan_map", _vp),
+        ("nrow", _i64), ("nchan", _i32), ("ncorr", _i32),
+        ("chan_equidistant", _i32),
+        ("bda_map", _vp), ("bda_len", _i64), ("block_start", _vp), ("nblocks", _i64),
+        ("sparsification", _vp),
+        ("uvw_dt", _vp), ("dt", _f64), ("dnu", _f64), ("do_tsmear", _i32), ("do_fsmear", _i32),
+    ]
+
+
+class Jones(C.Structure):
+    _fields_ = [
+        ("mode", _i32),
+        ("kms", _vp), ("kms_dims", _i32 * 4), ("kms_tmap", _vp), ("kms_cmap", _vp),
+        ("beam", _vp), ("beam_dims", _i32 * 4), ("beam_tmap", _vp), ("beam_cmap", _vp),
+        ("a0", _vp), ("a1", _vp),
+        ("interp_coefs", _vp), ("interp_mode", _i32),
+        ("apply_amp", _i32), ("apply_phase", _i32), ("scale_jones", _i32),
+        ("calib_error", _f64), ("wavelength_mean", _f64),
+    ]
+
+
+class Pol(C.Structure):
+    _fields_ = [("ncorr", _i32), ("npol", _i32), ("corr_ids", _i32 * 4), ("stokes_ids", _i32 * 4)]
+
+
+# Entry points declared in include/ddfg.h, with their ctypes signatures.
+SIGNATURES = {
+    "ddfg_version": (C.c_int, []),
+    "ddfg_last_error": (C.c_int, [C.c_char_p, C.c_int]),
+    "ddfg_bda_plan_workspace_size": (C.c_size_t, [_i64]),
+    "ddfg_bda_plan": (C.c_int, [_vp, _i64, _i64, _i64, _i32, _vp, _vp, C.c_size_t, _vp]),
+    "ddfg_grid": (C.c_int, [C.POINTER(VisSet), C.POINTER(Jones), C.POINTER(Pol), C.POINTER(Facet), C.c_int,
+                            C.c_int, _vp]),
+    "ddfg_degrid": (C.c_int, [C.POINTER(VisSet), C.POINTER(Jones), C.POINTER(Pol), C.POINTER(Facet), C.c_int,
+                              _vp]),
+}
+
+_lock = threading.Lock()
+_lib = None
+
+
+class DDFGError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"ddfg error {code}: {msg}")
+        self.code = code
+        self.msg = msg
+
+
+def lib_path() -> str:
+    return _build.LIB
+
+
+def lib():
+    """Load (building if needed) libddfg.so; raise if it cannot be loaded."""
+    global _lib
+    with _lock:
+        if _lib is None:
+            path = _build.LIB
+            if not os.path.exists(path):
+                _build.build()
+            # torch first, so the library binds to the CUDA runtime torch already loaded.
+            import torch  # noqa: F401
+            h = C.CDLL(path, mode=C.RTLD_GLOBAL)
+            for name, (res, args) in SIGNATURES.items():
+                fn = getattr(h, name)
+                fn.restype = res
+                fn.argtypes = args
+            _lib = h
+    return _lib
+
+
+def last_error() -> str:
+    buf = C.create_string_buffer(512)
+    lib().ddfg_last_error(buf, 512)
+    return buf.value.decode(errors="replace")
+
+
+def check(rc: int):
+    if rc != DDFG_OK:
+        msg = last_error()
+        if rc == DDFG_EUNSUPPORTED:
+            raise ValueError(msg)
+        raise DDFGError(rc, msg)
+    return rc

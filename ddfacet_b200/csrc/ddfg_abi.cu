@@ -1,0 +1,221 @@
+// C entry points of libddfg.so: argument checks, correlation/Stokes dispatch, error reporting.
+//
+// The dispatch tables restate pyGridderWPol / pyDeGridderWPol (DDFacet/Gridder/
+// GridderSmearPols.cc:98-209 and :234-348): the same accepted (correlations, Stokes)
+// combinations, the same quirk that gridding (I, U) from linear feeds uses the (I, Q) policy
+// (GridderSmearPols.cc:142-143), and the same error texts.
+#include <cuda_runtime.h>
+#include <stdarg.h>
+#include <stdio.h>
+#include <string.h>
+
+#include "ddfg_common.cuh"
+#include "ddfg_internal.h"
+
+using namespace ddfg;
+
+namespace {
+thread_local char g_err[512] = "";
+
+enum Corr { C_BAD = -1, C_I = 0, C_LIN2, C_CIRC2, C_LIN4, C_CIRC4 };
+
+int corr_set(const ddfg_pol *p) {
+  const int *c = p->corr_ids;
+  if (p->ncorr == 1 && c[0] == 1) return C_I;
+  if (p->ncorr == 2 && c[0] == 9 && c[1] == 12) return C_LIN2;
+  if (p->ncorr == 2 && c[0] == 5 && c[1] == 8) return C_CIRC2;
+  if (p->ncorr == 4 && c[0] == 9 && c[1] == 10 && c[2] == 11 && c[3] == 12) return C_LIN4;
+  if (p->ncorr == 4 && c[0] == 5 && c[1] == 6 && c[2] == 7 && c[3] == 8) return C_CIRC4;
+  return C_BAD;
+}
+
+// Stokes set as a string of letters, e.g. "IQUV".
+void stokes_str(const ddfg_pol *p, char *out) {
+  static const char *names = "?IQUV";
+  int n = 0;
+  for (int i = 0; i < p->npol && i < 4; ++i) {
+    const int id = p->stokes_ids[i];
+    out[n++] = (id >= 1 && id <= 4) ? names[id] : '?';
+  }
+  out[n] = 0;
+}
+
+bool corr_ids_ok(const ddfg_pol *p) {
+  if (p->ncorr < 1 || p->ncorr > 4) return false;
+  for (int i = 0; i < p->ncorr; ++i) {
+    const int id = p->corr_ids[i];
+    if (!((id >= 5 && id <= 12) || id == 1)) return false;
+  }
+  return true;
+}
+
+int grid_policy(const ddfg_pol *p) {
+  char s[8];
+  stokes_str(p, s);
+  switch (corr_set(p)) {
+    case C_LIN4:
+      if (!strcmp(s, "I")) return G_I_LIN4;
+      if (!strcmp(s, "Q")) return G_Q_LIN4;
+      if (!strcmp(s, "U")) return G_U_LIN4;
+      if (!strcmp(s, "V")) return G_V_LIN4;
+      if (!strcmp(s, "IQ")) return G_IQ_LIN4;
+      if (!strcmp(s, "IU")) return G_IQ_LIN4;  // GridderSmearPols.cc:142-143
+      if (!strcmp(s, "IV")) return G_IV_LIN4;
+      if (!strcmp(s, "QU")) return G_QU_LIN4;
+      if (!strcmp(s, "IQU")) return G_IQU_LIN4;
+      if (!strcmp(s, "IQUV")) return G_IQUV_LIN4;
+      break;
+    case C_CIRC4:
+      if (!strcmp(s, "I")) return G_I_CIRC4;
+      if (!strcmp(s, "IQ")) return G_IQ_CIRC4;
+      if (!strcmp(s, "IU")) return G_IU_CIRC4;
+      if (!strcmp(s, "IV")) return G_IV_CIRC4;
+      if (!strcmp(s, "QU")) return G_QU_CIRC4;
+      if (!strcmp(s, "IQU")) return G_IQU_CIRC4;
+      if (!strcmp(s, "IQUV")) return G_IQUV_CIRC4;
+      break;
+    case C_LIN2:
+      if (!strcmp(s, "I")) return G_I_LIN2;
+      if (!strcmp(s, "IQ")) return G_IQ_LIN2;
+      break;
+    case C_CIRC2:
+      if (!strcmp(s, "I")) return G_I_CIRC2;
+      if (!strcmp(s, "IV")) return G_IV_CIRC2;
+      break;
+    case C_I:
+      if (!strcmp(s, "I")) return G_I_FROM_I;
+      break;
+    default: break;
+  }
+  return -1;
+}
+
+int degrid_policy(const ddfg_pol *p) {
+  char s[8];
+  stokes_str(p, s);
+  const int c = corr_set(p);
+  if (!strcmp(s, "I")) {
+    if (c == C_LIN4 || c == C_LIN2 || c == C_CIRC4 || c == C_CIRC2 || c == C_I) return D_DIAG_FROM_I;
+  } else if (!strcmp(s, "Q")) {
+    if (c == C_LIN4) return D_LIN4_FROM_Q;
+  } else if (!strcmp(s, "U")) {
+    if (c == C_LIN4) return D_LIN4_FROM_U;
+  } else if (!strcmp(s, "V")) {
+    if (c == C_LIN4) return D_LIN4_FROM_V;
+  } else if (!strcmp(s, "IQUV")) {
+    if (c == C_LIN4) return D_LIN4_FROM_IQUV;
+    if (c == C_CIRC4) return D_CIRC4_FROM_IQUV;
+  } else if (!strcmp(s, "IQ")) {
+    if (c == C_LIN4) return D_LIN4_FROM_IQ;
+    if (c == C_CIRC4) return D_CIRC4_FROM_IQ;
+    if (c == C_LIN2) return D_LIN2_FROM_IQ;
+  } else if (!strcmp(s, "IU")) {
+    if (c == C_LIN4) return D_LIN4_FROM_IU;
+    if (c == C_CIRC4) return D_CIRC4_FROM_IU;
+  } else if (!strcmp(s, "IV")) {
+    if (c == C_CIRC4) return D_CIRC4_FROM_IV;
+    if (c == C_LIN4) return D_LIN4_FROM_IV;
+    if (c == C_CIRC2) return D_CIRC2_FROM_IV;
+  } else if (!strcmp(s, "QU")) {
+    if (c == C_LIN4) return D_LIN4_FROM_QU;
+  } else if (!strcmp(s, "IQU")) {
+    if (c == C_LIN4) return D_LIN4_FROM_IQU;
+    if (c == C_CIRC4) return D_CIRC4_FROM_IQU;
+  }
+  return -1;
+}
+
+int check_common(const char *who, const ddfg_vis *vs, const ddfg_jones *js, const ddfg_pol *pol,
+                 const ddfg_facet *facets, int nfacets) {
+  if (!vs || !js || !pol || !facets) return ddfg_set_error(DDFG_EINVAL, "%s: null argument", who);
+  if (nfacets < 0 || nfacets > DDFG_MAX_FACETS)
+    return ddfg_set_error(DDFG_ESIZE, "%s: nfacets=%d outside [0, %d]", who, nfacets, DDFG_MAX_FACETS);
+  if (vs->ncorr != pol->ncorr) return ddfg_set_error(DDFG_EINVAL, "%s: vis has %d correlations, pol lists %d", who, vs->ncorr, pol->ncorr);
+  if (vs->nblocks > 0 && (!vs->vis || !vs->uvw || !vs->freqs || !vs->chan_map || !vs->bda_map || !vs->block_start))
+    return ddfg_set_error(DDFG_EINVAL, "%s: null visibility-set pointer", who);
+  if (js->mode < 0 || js->mode > 2) return ddfg_set_error(DDFG_EINVAL, "%s: Jones mode %d", who, js->mode);
+  if (js->mode != 0) {
+    if (!js->kms && !js->beam)
+      return ddfg_set_error(DDFG_EINVAL, "Jones matricies specified but neither E or DD Jones are applied. This is a bug!");
+    if (!js->a0 || !js->a1) return ddfg_set_error(DDFG_EINVAL, "%s: Jones without antenna arrays", who);
+    if (js->kms && (!js->kms_tmap || !js->kms_cmap)) return ddfg_set_error(DDFG_EINVAL, "%s: DD Jones maps missing", who);
+    if (js->beam && (!js->beam_tmap || !js->beam_cmap)) return ddfg_set_error(DDFG_EINVAL, "%s: beam Jones maps missing", who);
+    if (js->interp_mode == 1 && !js->interp_coefs) return ddfg_set_error(DDFG_EINVAL, "%s: interpolation coefficients missing", who);
+  }
+  for (int i = 0; i < nfacets; ++i) {
+    const ddfg_facet &f = facets[i];
+    if (!f.grid || !f.cf_data || !f.cf_offset || !f.cf_support)
+      return ddfg_set_error(DDFG_EINVAL, "%s: facet %d has a null grid or CF pointer", who, i);
+    if (f.nx <= 0 || f.ny <= 0 || f.nband <= 0 || f.npol <= 0 || f.nw <= 0 || f.overs <= 0)
+      return ddfg_set_error(DDFG_EINVAL, "%s: facet %d has a bad shape", who, i);
+    if (f.wmax == 0.) return ddfg_set_error(DDFG_EINVAL, "%s: facet %d has wmax = 0", who, i);
+  }
+  return DDFG_OK;
+}
+}  // namespace
+
+int ddfg_set_error(int code, const char *fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(g_err, sizeof(g_err), fmt, ap);
+  va_end(ap);
+  return code;
+}
+
+int ddfg_num_ctas(int ctas_per_sm) {
+  static thread_local int cached_dev = -1, cached_sms = 0;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return 148 * ctas_per_sm;
+  if (dev != cached_dev) {
+    int sms = 0;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0) sms = 148;
+    cached_dev = dev;
+    cached_sms = sms;
+  }
+  return cached_sms * ctas_per_sm;
+}
+
+extern "C" int ddfg_version(void) { return 1; }
+
+extern "C" int ddfg_last_error(char *buf, int len) {
+  if (!buf || len <= 0) return (int)strlen(g_err);
+  snprintf(buf, (size_t)len, "%s", g_err);
+  return (int)strlen(g_err);
+}
+
+extern "C" int ddfg_grid(const ddfg_vis *vs, const ddfg_jones *js, const ddfg_pol *pol, const ddfg_facet *facets,
+                         int nfacets, int dopsf, void *stream) {
+  g_err[0] = 0;
+  int rc = check_common("grid", vs, js, pol, facets, nfacets);
+  if (rc) return rc;
+  if (!corr_ids_ok(pol))
+    return ddfg_set_error(DDFG_EUNSUPPORTED, "Only accepts I,RR,RL,LR,LL,XX,XY,YX,YY as correlation input type");
+  for (int i = 0; i < pol->npol; ++i)
+    if (pol->stokes_ids[i] < 1 || pol->stokes_ids[i] > 4)
+      return ddfg_set_error(DDFG_EUNSUPPORTED, "Only accepts I,Q,U,V as polarization output type");
+  const int policy = grid_policy(pol);
+  if (policy < 0)
+    return ddfg_set_error(DDFG_EUNSUPPORTED, "Cannot convert input correlations to desired output Stokes parameters.");
+  if (vs->nblocks > 0 && (!vs->flags || !vs->weights))
+    return ddfg_set_error(DDFG_EINVAL, "grid: null flags or weights");
+  if (nfacets == 0 || vs->nblocks == 0) return DDFG_OK;
+  return ddfg_launch_grid(vs, js, facets, nfacets, policy, pol->npol, dopsf, ddfg_num_ctas(4), (cudaStream_t)stream);
+}
+
+extern "C" int ddfg_degrid(const ddfg_vis *vs, const ddfg_jones *js, const ddfg_pol *pol, const ddfg_facet *facets,
+                           int nfacets, void *stream) {
+  g_err[0] = 0;
+  int rc = check_common("degrid", vs, js, pol, facets, nfacets);
+  if (rc) return rc;
+  if (!corr_ids_ok(pol))
+    return ddfg_set_error(DDFG_EUNSUPPORTED, "Only accepts I,RR,RL,LR,LL,XX,XY,YX,YY as correlation output types");
+  const int policy = degrid_policy(pol);
+  if (policy < 0)
+    return ddfg_set_error(DDFG_EUNSUPPORTED, "Cannot convert input Stokes parameter to desired output correlations.");
+  for (int i = 0; i < nfacets; ++i)
+    if (facets[i].npol < pol->npol)
+      return ddfg_set_error(DDFG_EINVAL, "degrid: facet %d grid has %d Stokes planes, %d needed", i, facets[i].npol,
+                            pol->npol);
+  if (nfacets == 0 || vs->nblocks == 0) return DDFG_OK;
+  return ddfg_launch_degrid(vs, js, facets, nfacets, policy, pol->npol, ddfg_num_ctas(4), (cudaStream_t)stream);
+}

@@ -1,0 +1,153 @@
+/*
+ * ddfg.h -- C ABI of the B200 facet gridder/degridder (libddfg.so).
+ *
+ * Plain C: every argument is a pointer, an integer or a double.  Every data pointer is a
+ * DEVICE pointer (CUDA global memory on the current device) unless a comment says "host".
+ * Calls are asynchronous on the given stream (cudaStream_t passed as void*; NULL = legacy
+ * default stream); they never allocate device memory and never synchronise.  Every entry point
+ * returns DDFG_OK (0) or a negative DDFG_E* code; ddfg_last_error() then gives the message of the
+ * failing call on this host thread.
+ *
+ * Arrays follow the reference's numpy layouts (C order):
+ *   grid     complex64 [nband][npol][ny][nx]
+ *   vis      complex64 [nrow][nchan][ncorr]
+ *   uvw      float64   [nrow][3]           (metres)
+ *   flags    uint8     [nrow][nchan][ncorr] (numpy bool)
+ *   weights  float32   [nrow][nchan]
+ *   BDA map  int32     [2 + NB + sum_b NRowBlocks[b]]  (DDFacet's packed block map)
+ *   Jones    complex64 [nt][nd][na][nch][2][2]
+ *   CF       complex64, each plane [S*OverS][S*OverS] re-ordered as [OverS][OverS][S][S]
+ */
+#ifndef DDFG_H
+#define DDFG_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DDFG_OK 0
+#define DDFG_EINVAL (-1)       /* bad argument (null pointer, bad shape)                  */
+#define DDFG_EUNSUPPORTED (-2) /* correlation / Stokes combination not handled            */
+#define DDFG_ECUDA (-3)        /* a CUDA runtime or cuFFT call failed                     */
+#define DDFG_EMAP (-4)         /* malformed BDA block map (row or channel out of range)   */
+#define DDFG_ESIZE (-5)        /* a size exceeds a documented maximum                     */
+
+/* Maximum number of facets one ddfg_grid / ddfg_degrid call may take. */
+#define DDFG_MAX_FACETS 1024
+/* Facets whose descriptors travel in one kernel launch (the rest go in further launches). */
+#define DDFG_FACETS_PER_LAUNCH 16
+
+/* One facet: its grid, geometry, W-projection tables and outputs.
+ * Replaces the per-facet arguments of pyGridderWPol / pyDeGridderWPol
+ * (DDFacet/Gridder/GridderSmearPols.cc:76-97, 212-233): grid, sumwt, Lcfs, LcfsConj, WInfos,
+ * increment, Lmaps[1] (FacetInfos) and LJones[6], LJones[8], LJones[17], LJones[18]. */
+typedef struct ddfg_facet {
+  void *grid;                  /* complex64 [nband][npol][ny][nx]                         */
+  int32_t nband, npol, ny, nx; /* grid shape                                              */
+  double incr_x, incr_y;       /* increment[0..1] in radians ([-cell, +cell])             */
+  double cu, cv, l0, m0;       /* FacetInfos[0..3]: uvw shift and facet centre            */
+  /* W-projection tables.  Plane p < nw is Lcfs[p] (used when the block's mean w > 0),
+   * plane nw + p is LcfsConj[p] (used when w <= 0).  cf_offset gives each plane's first
+   * complex element in cf_data; cf_support its support S (plane side = S * overs).        */
+  const void *cf_data;
+  const int64_t *cf_offset;    /* [2*nw] */
+  const int32_t *cf_support;   /* [2*nw] */
+  int32_t nw, overs;
+  double ref_wave, wmax;       /* WInfos[0], WInfos[1]                                    */
+  int32_t idir_kms, idir_beam; /* Jones direction of this facet (LJones[6][0], [8][0])    */
+  double decorr_l, decorr_m;   /* LSmearing[5..6]: lm at which smearing is evaluated      */
+  /* Outputs of ddfg_grid, accumulated (+=), float64; NULL to skip. */
+  double *sumwt;               /* [nband][npol]   (sumwt)                                 */
+  double *sumjones;            /* [2][nband]      (LJones[17])                            */
+  double *sumjones_chan;       /* [2][nchan]      (LJones[18])                            */
+} ddfg_facet;
+
+/* The visibilities and everything indexed by row/channel (facet independent). */
+typedef struct ddfg_vis {
+  void *vis;                   /* complex64 [nrow][nchan][ncorr]; ddfg_degrid subtracts   */
+  const double *uvw;           /* [nrow][3]                                               */
+  const uint8_t *flags;        /* [nrow][nchan][ncorr]; only corr 0 is read (gridder.h:229)*/
+  const float *weights;        /* [nrow][nchan]                                           */
+  const double *freqs;         /* [nchan] Hz                                              */
+  double freq_mean;            /* mean of freqs[] (host value; gridder.h:164-171)         */
+  const int32_t *chan_map;     /* [nchan] visibility channel -> grid band                 */
+  int64_t nrow;
+  int32_t nchan, ncorr;
+  int32_t chan_equidistant;    /* LOptimisation[1]                                        */
+  const int32_t *bda_map;      /* packed block map                                        */
+  int64_t bda_len;             /* words in bda_map                                        */
+  const int64_t *block_start;  /* [nblocks] word index of each block's [ch0,ch1,rows...]  */
+  int64_t nblocks;
+  const uint8_t *sparsification; /* [nblocks] (gridding only) or NULL                     */
+  /* Smearing (LSmearing, DecorrelationHelper.cc:19-40); uvw_dt NULL disables it. */
+  const double *uvw_dt;        /* [nrow][3]                                               */
+  double dt, dnu;
+  int32_t do_tsmear, do_fsmear;
+} ddfg_vis;
+
+/* Direction-dependent Jones terms (LJones, ClassDDEGridMachine.py:665-677). */
+typedef struct ddfg_jones {
+  int32_t mode;                /* 0 none, 1 per visibility, 2 per BDA block (DoApplyJones)*/
+  const void *kms;             /* complex64 [nt][nd][na][nch][2][2] or NULL               */
+  int32_t kms_dims[4];         /* nt, nd, na, nch                                         */
+  const int32_t *kms_tmap;     /* [nrow] row -> Jones time slot                           */
+  const int32_t *kms_cmap;     /* [nchan] channel -> Jones channel                        */
+  const void *beam;            /* complex64 [nt][nd][na][nch][2][2] or NULL               */
+  int32_t beam_dims[4];
+  const int32_t *beam_tmap;
+  const int32_t *beam_cmap;
+  const int32_t *a0, *a1;      /* [nrow] antennas                                         */
+  const float *interp_coefs;   /* [nd] (interp_mode 1) or NULL                            */
+  int32_t interp_mode;         /* 0 nearest, 1 weighted                                   */
+  int32_t apply_amp, apply_phase, scale_jones;
+  double calib_error;          /* radians                                                 */
+  double wavelength_mean;      /* mean over channels of c/nu                              */
+} ddfg_jones;
+
+/* Correlation and Stokes ids use casacore's numbering: I=1 Q=2 U=3 V=4 RR=5 RL=6 LR=7 LL=8
+ * XX=9 XY=10 YX=11 YY=12 (DDFacet/Data/ClassStokes.py:39). */
+typedef struct ddfg_pol {
+  int32_t ncorr, npol;
+  int32_t corr_ids[4];
+  int32_t stokes_ids[4];
+} ddfg_pol;
+
+/* Library and device checks. */
+int ddfg_version(void);
+int ddfg_last_error(char *buf, int len);
+
+/* Bytes of device scratch ddfg_bda_plan needs for a map of nblocks blocks. */
+size_t ddfg_bda_plan_workspace_size(int64_t nblocks);
+
+/* Reads the map's block sizes, writes the word index of every block record into block_start
+ * (device, int64 [nblocks]) and checks that the header's block count is nblocks, every block
+ * lies inside the map, 0 <= ch0 <= ch1 <= nchan and every row is in [0, nrow).  A plan call,
+ * not a hot one: it synchronises the stream to read the check's result, and returns DDFG_EMAP
+ * for a malformed map.  Replaces the sequential block walk of gridder.h:144-148, 185-190 and
+ * degridder.h:107-136. */
+int ddfg_bda_plan(const int32_t *bda_map, int64_t bda_len, int64_t nblocks, int64_t nrow, int32_t nchan,
+                  int64_t *block_start, void *workspace, size_t workspace_bytes, void *stream);
+
+/* Grid the visibility set onto every facet's grid (accumulating), with W-projection, facet
+ * phase shift, per-antenna Jones, smearing and corr->Stokes conversion.
+ * Replaces pyGridderWPol32 (DDFacet/Gridder/GridderSmearPols.cc:76-209, gridder.h:78-377),
+ * called once per facet by ClassDDEGridMachine.put (ClassDDEGridMachine.py:681-861).
+ * facets: HOST array of nfacets descriptors (copied into the launches). */
+int ddfg_grid(const ddfg_vis *vs, const ddfg_jones *js, const ddfg_pol *pol,
+              const ddfg_facet *facets, int nfacets, int dopsf, void *stream);
+
+/* Predict every facet's model grid and SUBTRACT the prediction from vs->vis in place.
+ * Replaces pyDeGridderWPol (GridderSmearPols.cc:212-348, degridder.h:55-267), called by
+ * ClassDDEGridMachine.get (ClassDDEGridMachine.py:922-1152).  The reference serialises the
+ * subtraction of concurrent facets with named semaphores (Semaphores.cc:27-29); here every
+ * facet of a call is applied by the warp that owns the block, so the result is deterministic. */
+int ddfg_degrid(const ddfg_vis *vs, const ddfg_jones *js, const ddfg_pol *pol,
+                const ddfg_facet *facets, int nfacets, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* DDFG_H */
