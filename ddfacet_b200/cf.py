@@ -24,6 +24,7 @@ the last ulp; the CF tables are then uploaded once and stay resident on the GPU.
 """
 from __future__ import annotations
 
+import functools
 import itertools
 import math
 
@@ -92,6 +93,13 @@ def zero_pad(a, outshape):
     return b
 
 
+@functools.lru_cache(maxsize=64)
+def _taper_cached(support, npix):
+    z = SpheroidalTaper(support)._taper(npix)
+    z.setflags(write=False)
+    return z
+
+
 class SpheroidalTaper:
     """``SpheMachine`` (ModCF.py:87-172) for the "Sphe" type."""
 
@@ -108,7 +116,11 @@ class SpheroidalTaper:
         self.small_cf = cf
 
     def taper(self, npix):
-        """The image-plane taper ``ifzfCF`` of side ``npix`` (ModCF.py:120-170)."""
+        """The image-plane taper ``ifzfCF`` of side ``npix`` (ModCF.py:120-170); memoised per
+        (support, npix) since it does not depend on the facet."""
+        return _taper_cached(self.support, int(npix)).copy()
+
+    def _taper(self, npix):
         z = ifft2c(zero_pad(self.small_fcf, npix))
         # ModCF.py:170 compares complex values lexicographically (real part first).
         neg = (z.real < 0) | ((z.real == 0) & (z.imag < 0))

@@ -1,0 +1,159 @@
+"""The benchmark workloads, built from seeded synthetic data directly in device memory.
+
+``multifacet_dde`` is the multi-facet direction-dependent imaging workload: a 4096^2 image at
+1.5 arcsec in 9 x 9 regular facets (padding 1.7, 735^2 padded grids), 64 antennas uniform in a
+disk of 4 km radius (8 km across) at latitude +34 deg observing dec +40 deg for 4 h at 8 s
+(1800 dumps, 2016 baselines, 3.63 M rows), 64 channels over 0.90-1.67 GHz, 4 linear
+correlations gridded to Stokes I, 200 power-law point sources plus 1 mJy noise, per-facet
+per-antenna 2x2 Jones in 5-min slots (identity + 0.1 complex Gaussian), W-projection with
+32 planes, supports from 7, oversampling 11.  Every (row, channel) is its own block (no BDA).
+
+``plain_small`` is the single-facet, Stokes-I, 1024^2 image case (27 antennas in a 20 km
+radius, 2 h at 10 s, 16 channels over 1.30-1.45 GHz, 8 w-planes, support 7).
+
+``scale`` shrinks the number of dumps (and so rows) for quick runs; 1.0 is the full size.
+"""
+from __future__ import annotations
+
+import concurrent.futures as cfut
+from dataclasses import dataclass, field
+from typing import List, Optional
+
+import numpy as np
+import torch
+
+from . import bda, cf, device as D, geometry, synth
+
+C_LIGHT = 299792458.0
+
+
+@dataclass
+class Workload:
+    name: str
+    vs: D.VisData
+    facets_grid: List[D.FacetGrid]      # residual grids (gridding target)
+    facets_model: List[D.FacetGrid]     # model grids (degridding source), same CF tables
+    jones: Optional[D.JonesData]
+    pol: object
+    nvis: int
+    nrow: int
+    nchan: int
+    ncorr: int
+    nfacets: int
+    host: dict = field(default_factory=dict)   # host copies for the end-to-end path
+    info: dict = field(default_factory=dict)
+
+
+def _gen_vis_gpu(uvw_d, freqs_d, l, m, s, ncorr, noise_sigma, seed, dev, row_chunk=1 << 16):
+    """Point-source visibilities + complex noise on the GPU (FP64 phase, complex64 result)."""
+    nrow = uvw_d.shape[0]
+    nchan = freqs_d.numel()
+    out = torch.empty((nrow, nchan, ncorr), dtype=torch.complex64, device=dev)
+    g = torch.Generator(device=dev)
+    g.manual_seed(seed)
+    lt = torch.tensor(l, dtype=torch.float64, device=dev)
+    mt = torch.tensor(m, dtype=torch.float64, device=dev)
+    nt = torch.sqrt(1 - lt ** 2 - mt ** 2) - 1
+    st = torch.tensor(s, dtype=torch.float32, device=dev)
+    fr = (freqs_d / C_LIGHT).to(torch.float64)
+    for r0 in range(0, nrow, row_chunk):
+        uu = uvw_d[r0:r0 + row_chunk]
+        acc = torch.zeros((uu.shape[0], nchan), dtype=torch.complex64, device=dev)
+        for k in range(lt.numel()):
+            ph = uu[:, 0] * lt[k] + uu[:, 1] * mt[k] + uu[:, 2] * nt[k]          # metres
+            turns = ph[:, None] * fr[None, :]
+            frac = (turns - torch.round(turns)).to(torch.float32)
+            acc += st[k] * torch.polar(torch.ones_like(frac), 2 * np.pi * frac)
+        noise = torch.randn((uu.shape[0], nchan, ncorr, 2), generator=g, device=dev) * noise_sigma
+        blk = torch.view_as_complex(noise.contiguous())
+        blk[:, :, 0] += acc
+        blk[:, :, ncorr - 1] += acc
+        out[r0:r0 + row_chunk] = blk
+    return out
+
+
+def _plain_map_gpu(A0, A1, nchan, dev):
+    """bda.plain_map built with device tensors (same words)."""
+    groups = bda._baseline_rows(A0, A1)
+    keys = sorted(groups.keys(), key=lambda k: "%d:%d" % k)
+    rows = np.concatenate([groups[k] for k in keys]).astype(np.int32)
+    nb = rows.size * nchan
+    rows_d = torch.from_numpy(rows).to(dev)
+    m = torch.empty(2 + nb + 3 * nb, dtype=torch.int32, device=dev)
+    m[0:2] = torch.from_numpy(bda._header(nb)).to(dev)
+    m[2:2 + nb] = 3
+    body = m[2 + nb:].view(nb, 3)
+    ch = torch.arange(nchan, dtype=torch.int32, device=dev).repeat(rows.size)
+    body[:, 0] = ch
+    body[:, 1] = ch + 1
+    body[:, 2] = rows_d.repeat_interleave(nchan)
+    return m
+
+
+def _wterms(args):
+    (cell, sup, nw, wmax, npix, freqs, overs, lm, i) = args
+    return cf.WTerms(Cell=cell, Sup=sup, Nw=nw, wmax=wmax, Npix=npix, Freqs=freqs, OverS=overs, lmShift=lm,
+                     IDFacet=i)
+
+
+def build_wterms(tess_facets, cell, sup, nw, wmax, npix, freqs, overs, threads=8):
+    args = [(cell, sup, nw, wmax, npix, freqs, overs, (f.l0, f.m0), f.index) for f in tess_facets]
+    with cfut.ThreadPoolExecutor(threads) as ex:
+        return list(ex.map(_wterms, args))
+
+
+def multifacet_dde(device=None, scale=1.0, seed=1002, nfacets_side=9, nchan=64, nw=32, with_jones=True,
+                   keep_host=True, nsrc=200):
+    dev = D._dev(device)
+    hours = 4.0 * scale
+    obs = synth.make_observation(seed, 64, 4000.0, 34.0, 40.0, hours, 8.0, nchan, 0.90e9, 1.67e9)
+    tess = geometry.regular_facets(4096, nfacets_side, 1.5, 1.7)
+    npix_pad = tess.npix_padded
+    cell = 1.5
+    wmax = float(np.max(np.abs(obs.uvw[:, 2]))) * 1.001
+    wts = build_wterms(tess.facets, cell, 7, nw, wmax, tess.npix_facet * 0 + npix_pad, obs.freqs, 11)
+    field_rad = tess.npix * tess.cell_rad / 2
+    l, m, s = synth.point_sky(seed + 1, nsrc, field_rad * 0.95, flux=("powerlaw", 1e-4, 1.0))
+    uvw_d = torch.from_numpy(obs.uvw).to(dev)
+    freqs_d = torch.from_numpy(obs.freqs).to(dev)
+    ncorr = 4
+    vis = _gen_vis_gpu(uvw_d, freqs_d, l, m, s, ncorr, 1e-3, seed + 2, dev)
+    nrow = obs.nrow
+    flags = torch.zeros((nrow, nchan, ncorr), dtype=torch.uint8, device=dev)
+    weights = torch.ones((nrow, nchan), dtype=torch.float32, device=dev)
+    chan_map = np.zeros(nchan, np.int32)
+    bmap = _plain_map_gpu(obs.A0, obs.A1, nchan, dev)
+    vs = D.VisData.create(vis, uvw_d, flags, weights, obs.freqs, chan_map, bmap, device=dev)
+    jd = None
+    if with_jones:
+        nt = int(np.ceil(hours * 3600 / 300.0))
+        J = synth.random_jones(seed + 3, nt, len(tess.facets), 64, 1, 0.1)
+        tmap = np.minimum(((obs.times - obs.times.min()) // 300.0).astype(np.int32), nt - 1)
+        jd = D.JonesData(mode=1, kms=torch.from_numpy(J).to(dev), kms_tmap=torch.from_numpy(tmap).to(dev),
+                         kms_cmap=torch.zeros(nchan, dtype=torch.int32, device=dev),
+                         a0=torch.from_numpy(obs.A0).to(dev), a1=torch.from_numpy(obs.A1).to(dev),
+                         wavelength_mean=float(np.mean(C_LIGHT / obs.freqs)))
+    fg, fm = [], []
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(seed + 4)
+    for f, wt in zip(tess.facets, wts):
+        tabs = D.CFTables.create(wt.Wplanes, wt.WplanesConj, 11, wt.RefWave, wt.wmax, device=dev)
+        incr = (-cell / 3600 * np.pi / 180, cell / 3600 * np.pi / 180)
+        g = torch.zeros((1, 1, npix_pad, npix_pad), dtype=torch.complex64, device=dev)
+        mg = torch.randn((1, 1, npix_pad, npix_pad, 2), generator=gen, device=dev)
+        mg = torch.view_as_complex(mg.contiguous()) * 1e-3
+        common = dict(cf=tabs, incr=incr, cu=wt.Cu, cv=wt.Cv, l0=f.l0, m0=f.m0, idir_kms=f.index, idir_beam=0)
+        fg.append(D.FacetGrid(grid=g, sumwt=torch.zeros((1, 1), dtype=torch.float64, device=dev),
+                              sumjones=torch.zeros((2, 1), dtype=torch.float64, device=dev),
+                              sumjones_chan=torch.zeros((2, nchan), dtype=torch.float64, device=dev), **common))
+        fm.append(D.FacetGrid(grid=mg, **common))
+    pol = D.make_pol([9, 10, 11, 12], [1])
+    w = Workload("multifacet_dde", vs, fg, fm, jd, pol, nvis=nrow * nchan, nrow=nrow, nchan=nchan, ncorr=ncorr,
+                 nfacets=len(fg))
+    w.info = dict(npix=tess.npix, npix_facet=tess.npix_facet, npix_padded=npix_pad, nw=nw,
+                  supports=sorted(set(int(x) for x in wts[0].Sups)), wmax=wmax, nant=64, ntimes=obs.ntimes,
+                  nbl=obs.nbl)
+    w.host = {"obs": obs, "wterms": wts, "tess": tess, "chan_map": chan_map}
+    if keep_host:
+        w.host["vis"] = vis.cpu().pin_memory()
+    return w
