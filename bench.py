@@ -142,9 +142,10 @@ def cpu_reference(nfacets_total=81, nrow_frac=0.02, nprocs=None, seed=1002):
 # GPU arm
 # ------------------------------------------------------------------------------------------
 class ClockSampler:
-    def __init__(self, path):
+    def __init__(self, path, gpu_id=None):
         self.path = path
         self.p = None
+        self.gpu_id = gpu_id
 
     def __enter__(self):
         try:
@@ -153,7 +154,8 @@ class ClockSampler:
                 ["nvidia-smi", "--query-gpu=index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
                  "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
                  "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
-                 "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+                 "--format=csv,noheader,nounits", "-lms", "200"] + (["-i", self.gpu_id] if self.gpu_id else []),
+                stdout=self.f, stderr=subprocess.DEVNULL)
         except Exception:
             self.p = None
         return self
@@ -167,10 +169,10 @@ class ClockSampler:
                 self.p.kill()
             self.f.close()
 
-    def summary(self, gpu_index=0):
+    def summary(self):
         try:
             rows = [r.split(",") for r in open(self.path).read().strip().splitlines()]
-            rows = [[x.strip() for x in r] for r in rows if len(r) >= 9 and r[0].strip() == str(gpu_index)]
+            rows = [[x.strip() for x in r] for r in rows if len(r) >= 9]
             sm = [float(r[1]) for r in rows]
             mx = max(float(r[2]) for r in rows)
             names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
@@ -215,19 +217,32 @@ def run_gpu(args):
     w = configs.multifacet_dde(device=dev, scale=args.scale)
     torch.cuda.synchronize()
     t_build = time.perf_counter() - t_build
+    t_plan = time.perf_counter()
+    plan = D.SortPlan.build(w.vs, w.facets_grid, chunk=args.chunk)
+    torch.cuda.synchronize()
+    t_plan = time.perf_counter() - t_plan
     stream = torch.cuda.current_stream()
+    fpl = args.facets_per_launch
 
     def step(ev=None):
         for f in w.facets_grid:
             f.grid.zero_()
         if ev:
             ev[0].record(stream)
-        D.degrid(w.vs, w.facets_model, w.pol, w.jones)
+        D.degrid_sorted(w.vs, w.facets_model, w.pol, plan, w.jones, facets_per_launch=fpl)
         if ev:
             ev[1].record(stream)
-        D.grid(w.vs, w.facets_grid, w.pol, w.jones)
+        D.grid_sorted(w.vs, w.facets_grid, w.pol, plan, w.jones, facets_per_launch=fpl)
         if ev:
             ev[2].record(stream)
+
+    def plain_step():
+        # the same physics with one facet per launch, blocks in map order (direct kernels)
+        for fm, fg in zip(w.facets_model, w.facets_grid):
+            D.degrid(w.vs, [fm], w.pol, w.jones)
+        for fg in w.facets_grid:
+            fg.grid.zero_()
+            D.grid(w.vs, [fg], w.pol, w.jones)
 
     for _ in range(max(3, args.warmup)):
         step()
@@ -237,7 +252,13 @@ def run_gpu(args):
     evs = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(args.steps)]
     start = torch.cuda.Event(enable_timing=True)
     stop = torch.cuda.Event(enable_timing=True)
-    clk = ClockSampler(os.path.join(tempfile.gettempdir(), f"ddfg_clocks_{os.getpid()}.csv"))
+    gpu_id = None
+    try:
+        gpu_id = "GPU-" + str(torch.cuda.get_device_properties(dev).uuid).replace("GPU-", "")
+    except Exception:
+        cvd = os.environ.get("CUDA_VISIBLE_DEVICES", "")
+        gpu_id = cvd.split(",")[dev.index or 0] if cvd else None
+    clk = ClockSampler(os.path.join(tempfile.gettempdir(), f"ddfg_clocks_{os.getpid()}.csv"), gpu_id)
     with clk:
         torch.cuda.synchronize()
         start.record(stream)
@@ -290,6 +311,18 @@ def run_gpu(args):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_ms = float(t.item())
 
+    plain_ms = None
+    if args.plain:
+        plain_step()
+        torch.cuda.synchronize()
+        p0 = torch.cuda.Event(enable_timing=True)
+        p1 = torch.cuda.Event(enable_timing=True)
+        p0.record(stream)
+        plain_step()
+        p1.record(stream)
+        torch.cuda.synchronize()
+        plain_ms = p0.elapsed_time(p1)
+
     nvis = w.nvis
     value = world * nvis / (ms_step * 1e-3) / 1e6
     e2e_value = world * nvis / (e2e_ms * 1e-3) / 1e6
@@ -300,7 +333,7 @@ def run_gpu(args):
     G = w.info["npix_padded"]
     cf_bytes = sum(int(f.cf.data.numel()) * 8 for f in w.facets_grid)
     jones_bytes = int(w.jones.kms.numel()) * 8 if w.jones is not None else 0
-    launches_per_call = math.ceil(F / 16)
+    launches_per_call = math.ceil(F / (fpl if fpl > 0 else 16))
     grid_bytes = (launches_per_call * (nvis * (K * 8 + K + 4) + w.nrow * 24 + jones_bytes)
                   + F * G * G * 8 * 2 + cf_bytes // 2)
     degrid_bytes = (launches_per_call * (nvis * (K * 16) + w.nrow * 24 + jones_bytes)
@@ -337,6 +370,12 @@ def run_gpu(args):
             "scale": args.scale,
         },
         "kernels_ms": {"degrid_call": round(degrid_ms, 3), "grid_call": round(grid_ms, 3)},
+        "plain": (None if plain_ms is None else
+                  {"ms_per_step": round(plain_ms, 1), "value": round(world * nvis / (plain_ms * 1e-3) / 1e6, 3),
+                   "what": "direct kernels, blocks in map order, one facet per launch, global atomics",
+                   "batched_speedup": round(plain_ms / ms_step, 2)}),
+        "plan": {"blocks": int(plan.st.nplanned), "chunk": args.chunk, "build_s": round(t_plan, 2),
+                 "facets_per_launch": fpl},
         "roofline": {
             "bound": "hbm", "kernel": dom, "achieved": round(achieved, 2), "peak": hbm_peak, "unit": "GB/s",
             "frac": round(achieved / hbm_peak, 5), "peak_kind": peak_kind, "traffic": None,
@@ -347,7 +386,7 @@ def run_gpu(args):
         "e2e": {"value": round(e2e_value, 3), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h), "ms_per_step": round(e2e_ms, 3)},
         "gpu_launches": args.steps * 2 * launches_per_call,
-        "clocks": clk.summary(dev.index or 0),
+        "clocks": clk.summary(),
         "setup_s": round(t_build, 1),
     }
     if world > 1:
@@ -396,6 +435,9 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--scale", type=float, default=1.0)
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
+    ap.add_argument("--plain", action="store_true", help="also time the one-facet-per-launch direct path")
+    ap.add_argument("--chunk", type=int, default=1024)
+    ap.add_argument("--facets-per-launch", dest="facets_per_launch", type=int, default=8)
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

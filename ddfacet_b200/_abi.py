@@ -35,6 +35,7 @@ class Facet(C.Structure):
         ("cu", _f64), ("cv", _f64), ("l0", _f64), ("m0", _f64),
         ("cf_data", _vp), ("cf_offset", _vp), ("cf_support", _vp),
         ("nw", _i32), ("overs", _i32),
+        ("max_support", _i32),
         ("ref_wave", _f64), ("wmax", _f64),
         ("idir_kms", _i32), ("idir_beam", _i32),
         ("decorr_l", _f64), ("decorr_m", _f64),
@@ -46,6 +47,7 @@ class VisSet(C.Structure):
     _fields_ = [
         ("vis", _vp), ("uvw", _vp), ("flags", _vp), ("weights", _vp), ("freqs", _vp),
         ("freq_mean", _f64),
+        ("recip_wvl", _vp),
         ("chan_map", _vp),
         ("nrow", _i64), ("nchan", _i32), ("ncorr", _i32),
         ("chan_equidistant", _i32),
@@ -67,6 +69,10 @@ class Jones(C.Structure):
     ]
 
 
+class SortPlan(C.Structure):
+    _fields_ = [("perm", _vp), ("chunk", _i32), ("gref", _i32), ("nplanned", _i64)]
+
+
 class Pol(C.Structure):
     _fields_ = [("ncorr", _i32), ("npol", _i32), ("corr_ids", _i32 * 4), ("stokes_ids", _i32 * 4)]
 
@@ -81,6 +87,13 @@ SIGNATURES = {
                             C.c_int, _vp]),
     "ddfg_degrid": (C.c_int, [C.POINTER(VisSet), C.POINTER(Jones), C.POINTER(Pol), C.POINTER(Facet), C.c_int,
                               _vp]),
+    "ddfg_sort_plan_workspace_size": (C.c_size_t, [_i64]),
+    "ddfg_sort_plan_build": (C.c_int, [C.POINTER(VisSet), C.POINTER(Facet), C.POINTER(SortPlan), _vp, C.c_size_t,
+                                       _vp]),
+    "ddfg_grid_sorted": (C.c_int, [C.POINTER(VisSet), C.POINTER(Jones), C.POINTER(Pol), C.POINTER(Facet), C.c_int,
+                                   C.c_int, C.POINTER(SortPlan), C.c_int, C.c_int, _vp]),
+    "ddfg_degrid_sorted": (C.c_int, [C.POINTER(VisSet), C.POINTER(Jones), C.POINTER(Pol), C.POINTER(Facet),
+                                     C.c_int, C.POINTER(SortPlan), C.c_int, _vp]),
 }
 
 _lock = threading.Lock()

@@ -149,7 +149,12 @@ int check_common(const char *who, const ddfg_vis *vs, const ddfg_jones *js, cons
     if (f.nx <= 0 || f.ny <= 0 || f.nband <= 0 || f.npol <= 0 || f.nw <= 0 || f.overs <= 0)
       return ddfg_set_error(DDFG_EINVAL, "%s: facet %d has a bad shape", who, i);
     if (f.wmax == 0.) return ddfg_set_error(DDFG_EINVAL, "%s: facet %d has wmax = 0", who, i);
+    if (f.max_support <= 0 || f.max_support > 63)
+      return ddfg_set_error(DDFG_EINVAL, "%s: facet %d max_support %d outside [1, 63]", who, i, f.max_support);
   }
+  if (vs->ncorr == 4 && ((uintptr_t)vs->vis & 15))
+    return ddfg_set_error(DDFG_EINVAL, "%s: 4-correlation visibilities must be 16-byte aligned", who);
+  if ((uintptr_t)vs->vis & 7) return ddfg_set_error(DDFG_EINVAL, "%s: visibilities must be 8-byte aligned", who);
   return DDFG_OK;
 }
 }  // namespace
@@ -183,9 +188,9 @@ extern "C" int ddfg_last_error(char *buf, int len) {
   return (int)strlen(g_err);
 }
 
-extern "C" int ddfg_grid(const ddfg_vis *vs, const ddfg_jones *js, const ddfg_pol *pol, const ddfg_facet *facets,
-                         int nfacets, int dopsf, void *stream) {
-  g_err[0] = 0;
+namespace {
+int grid_checks(const ddfg_vis *vs, const ddfg_jones *js, const ddfg_pol *pol, const ddfg_facet *facets, int nfacets,
+                int *policy) {
   int rc = check_common("grid", vs, js, pol, facets, nfacets);
   if (rc) return rc;
   if (!corr_ids_ok(pol))
@@ -193,11 +198,74 @@ extern "C" int ddfg_grid(const ddfg_vis *vs, const ddfg_jones *js, const ddfg_po
   for (int i = 0; i < pol->npol; ++i)
     if (pol->stokes_ids[i] < 1 || pol->stokes_ids[i] > 4)
       return ddfg_set_error(DDFG_EUNSUPPORTED, "Only accepts I,Q,U,V as polarization output type");
-  const int policy = grid_policy(pol);
-  if (policy < 0)
+  *policy = grid_policy(pol);
+  if (*policy < 0)
     return ddfg_set_error(DDFG_EUNSUPPORTED, "Cannot convert input correlations to desired output Stokes parameters.");
-  if (vs->nblocks > 0 && (!vs->flags || !vs->weights))
-    return ddfg_set_error(DDFG_EINVAL, "grid: null flags or weights");
+  if (vs->nblocks > 0 && (!vs->flags || !vs->weights)) return ddfg_set_error(DDFG_EINVAL, "grid: null flags or weights");
+  return DDFG_OK;
+}
+int degrid_checks(const ddfg_vis *vs, const ddfg_jones *js, const ddfg_pol *pol, const ddfg_facet *facets,
+                  int nfacets, int *policy) {
+  int rc = check_common("degrid", vs, js, pol, facets, nfacets);
+  if (rc) return rc;
+  if (!corr_ids_ok(pol))
+    return ddfg_set_error(DDFG_EUNSUPPORTED, "Only accepts I,RR,RL,LR,LL,XX,XY,YX,YY as correlation output types");
+  *policy = degrid_policy(pol);
+  if (*policy < 0)
+    return ddfg_set_error(DDFG_EUNSUPPORTED, "Cannot convert input Stokes parameter to desired output correlations.");
+  for (int i = 0; i < nfacets; ++i)
+    if (facets[i].npol < pol->npol)
+      return ddfg_set_error(DDFG_EINVAL, "degrid: facet %d grid has %d Stokes planes, %d needed", i, facets[i].npol,
+                            pol->npol);
+  return DDFG_OK;
+}
+int max_sup(const ddfg_facet *facets, int n) {
+  int m = 1;
+  for (int i = 0; i < n; ++i) m = facets[i].max_support > m ? facets[i].max_support : m;
+  return m;
+}
+int plan_checks(const ddfg_sort_plan *plan, const ddfg_vis *vs) {
+  if (!plan || !plan->perm) return ddfg_set_error(DDFG_EINVAL, "sorted: null plan");
+  if (plan->gref <= 0 || plan->nplanned < 0) return ddfg_set_error(DDFG_EINVAL, "sorted: plan not built");
+  if (plan->nplanned > vs->nblocks) return ddfg_set_error(DDFG_EINVAL, "sorted: plan covers more blocks than the map has");
+  return DDFG_OK;
+}
+}  // namespace
+
+extern "C" int ddfg_grid_sorted(const ddfg_vis *vs, const ddfg_jones *js, const ddfg_pol *pol, const ddfg_facet *facets,
+                                int nfacets, int dopsf, const ddfg_sort_plan *plan, int compensated,
+                                int facets_per_launch, void *stream) {
+  g_err[0] = 0;
+  int policy = -1;
+  int rc = grid_checks(vs, js, pol, facets, nfacets, &policy);
+  if (rc) return rc;
+  rc = plan_checks(plan, vs);
+  if (rc) return rc;
+  if (nfacets == 0 || vs->nblocks == 0) return DDFG_OK;
+  return ddfg_launch_grid_sorted(vs, js, facets, nfacets, policy, pol->npol, dopsf, plan, compensated,
+                                 max_sup(facets, nfacets), facets_per_launch, (cudaStream_t)stream);
+}
+
+extern "C" int ddfg_degrid_sorted(const ddfg_vis *vs, const ddfg_jones *js, const ddfg_pol *pol,
+                                  const ddfg_facet *facets, int nfacets, const ddfg_sort_plan *plan,
+                                  int facets_per_launch, void *stream) {
+  g_err[0] = 0;
+  int policy = -1;
+  int rc = degrid_checks(vs, js, pol, facets, nfacets, &policy);
+  if (rc) return rc;
+  rc = plan_checks(plan, vs);
+  if (rc) return rc;
+  if (nfacets == 0 || vs->nblocks == 0) return DDFG_OK;
+  return ddfg_launch_degrid_sorted(vs, js, facets, nfacets, policy, pol->npol, plan, max_sup(facets, nfacets),
+                                   facets_per_launch, (cudaStream_t)stream);
+}
+
+extern "C" int ddfg_grid(const ddfg_vis *vs, const ddfg_jones *js, const ddfg_pol *pol, const ddfg_facet *facets,
+                         int nfacets, int dopsf, void *stream) {
+  g_err[0] = 0;
+  int policy = -1;
+  int rc = grid_checks(vs, js, pol, facets, nfacets, &policy);
+  if (rc) return rc;
   if (nfacets == 0 || vs->nblocks == 0) return DDFG_OK;
   return ddfg_launch_grid(vs, js, facets, nfacets, policy, pol->npol, dopsf, ddfg_num_ctas(4), (cudaStream_t)stream);
 }
@@ -205,17 +273,9 @@ extern "C" int ddfg_grid(const ddfg_vis *vs, const ddfg_jones *js, const ddfg_po
 extern "C" int ddfg_degrid(const ddfg_vis *vs, const ddfg_jones *js, const ddfg_pol *pol, const ddfg_facet *facets,
                            int nfacets, void *stream) {
   g_err[0] = 0;
-  int rc = check_common("degrid", vs, js, pol, facets, nfacets);
+  int policy = -1;
+  int rc = degrid_checks(vs, js, pol, facets, nfacets, &policy);
   if (rc) return rc;
-  if (!corr_ids_ok(pol))
-    return ddfg_set_error(DDFG_EUNSUPPORTED, "Only accepts I,RR,RL,LR,LL,XX,XY,YX,YY as correlation output types");
-  const int policy = degrid_policy(pol);
-  if (policy < 0)
-    return ddfg_set_error(DDFG_EUNSUPPORTED, "Cannot convert input Stokes parameter to desired output correlations.");
-  for (int i = 0; i < nfacets; ++i)
-    if (facets[i].npol < pol->npol)
-      return ddfg_set_error(DDFG_EINVAL, "degrid: facet %d grid has %d Stokes planes, %d needed", i, facets[i].npol,
-                            pol->npol);
   if (nfacets == 0 || vs->nblocks == 0) return DDFG_OK;
   return ddfg_launch_degrid(vs, js, facets, nfacets, policy, pol->npol, ddfg_num_ctas(4), (cudaStream_t)stream);
 }

@@ -14,12 +14,13 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
-#include "../../include/ddfg.h"
+#include "ddfg.h"
 
 namespace ddfg {
 
 constexpr double kC = 299792458.0;                      // common.h:9
 constexpr double kPi = 3.141592653589793238462643383279502884197;
+constexpr double kInvC = 1.0 / 299792458.0;  // phase arguments only; index arithmetic divides by kC
 
 // ----------------------------------------------------------------------------------------
 // complex helpers (float2 = complex64)
@@ -152,13 +153,13 @@ __device__ __forceinline__ void norm_jones(M2 &j, const ddfg_jones &js, double u
 struct JonesCache {
   int ant0, ant1, tk, ck, tb, cb;
   double uk, vk;
-  M2 j0, j1, j0h, j1h;
+  M2 j0, j1;
   float bb;
   __device__ __forceinline__ void reset() {
     ant0 = ant1 = -1;
     tk = ck = tb = cb = -1;
     uk = vk = 0.;
-    j0 = j1 = j0h = j1h = m2_unity();
+    j0 = j1 = m2_unity();
     bb = 1.f;
   }
   // Returns true when J0/J1 changed (JonesServer.cc:193-298).
@@ -209,8 +210,6 @@ struct JonesCache {
       j1 = b;
       const float t = (cabs2(j0.v[0]) * cabs2(j1.v[0]) + cabs2(j0.v[3]) * cabs2(j1.v[3])) * 0.5f;
       bb = t * t;
-      j0h = m2_herm(j0);
-      j1h = m2_herm(j1);
     }
     return changed;
   }
@@ -329,6 +328,7 @@ struct BlockGeom {
   int locx, locy;  // centre cell
   int sup;         // (S-1)/2
   int S;           // support
+  unsigned inv;    // ceil(65536 / S): t / S == (t * inv) >> 16 for every tap t < S*S (S <= 63)
   const float2 *cf;  // first tap of the [io][jo] sub-kernel (S*S taps, row-major sy, sx)
 };
 
@@ -365,8 +365,19 @@ __device__ __forceinline__ bool block_geometry(const ddfg_facet &f, double umean
   g.locy = (int)ly;
   g.sup = sup;
   g.S = S;
+  g.inv = (65536u + (unsigned)S - 1u) / (unsigned)S;
   g.cf = (const float2 *)f.cf_data + f.cf_offset[plane] + (int64_t)k * S * S;
   return true;
+}
+
+// Facet descriptors of a launch, copied to shared memory once per CTA: indexing them in the
+// kernel parameter space with a loop index would go through local memory.
+template <typename Pack>
+__device__ __forceinline__ void stage_facets(const Pack &pack, ddfg_facet *sf) {
+  const int words = pack.n * (int)(sizeof(ddfg_facet) / sizeof(int));
+  const int *src = (const int *)pack.f;
+  int *dst = (int *)sf;
+  for (int i = threadIdx.x; i < words; i += blockDim.x) dst[i] = src[i];
 }
 
 }  // namespace ddfg

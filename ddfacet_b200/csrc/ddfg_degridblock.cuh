@@ -1,0 +1,113 @@
+// The degridder's per-block steps (shared by the direct and the tile-sorted kernels):
+// block means and footprint (degridder.h:138-200) and the per-visibility correction and
+// subtraction (degridder.h:214-264).
+#pragma once
+#include "ddfg_common.cuh"
+
+namespace ddfg {
+
+struct FacetPackD {
+  ddfg_facet f[DDFG_FACETS_PER_LAUNCH];
+  int n;
+};
+
+struct DegridParams {
+  int policy;   // DegridPolicy
+  int nvispol;  // Stokes planes read from the model grid
+};
+
+struct DegridBlock {
+  int64_t start;
+  int nrows, ch0, ch1;
+  const int32_t *rows;
+  int gridchan;
+  double freqmean;
+};
+
+__device__ __forceinline__ void degrid_block_header(const ddfg_vis &vs, int64_t b, DegridBlock &d) {
+  d.start = vs.block_start[b];
+  d.nrows = vs.bda_map[2 + b] - 2;
+  d.ch0 = vs.bda_map[d.start];
+  d.ch1 = vs.bda_map[d.start + 1];
+  d.rows = vs.bda_map + d.start + 2;
+  d.gridchan = vs.chan_map[d.ch0 < vs.nchan ? d.ch0 : 0];
+  double fm = 0.;
+  for (int c = d.ch0; c < d.ch1; ++c) fm = dadd(fm, vs.freqs[c]);
+  const int nc = d.ch1 - d.ch0;
+  d.freqmean = (nc == 1) ? fm : fm / (double)nc;
+}
+
+// Footprint of block b on facet f; false when the reference skips it.
+__device__ __forceinline__ bool degrid_block_geom(const ddfg_vis &vs, const ddfg_facet &f, const DegridBlock &d,
+                                                  BlockGeom &g) {
+  if (d.ch1 <= d.ch0 || d.nrows <= 0) return false;
+  if (d.gridchan < 0 || d.gridchan >= f.nband) return false;
+  double um = 0., vm = 0., wm = 0.;
+  for (int inx = 0; inx < d.nrows; ++inx) {
+    const double *up = vs.uvw + 3 * (int64_t)d.rows[inx];
+    um = dadd(um, dadd(up[0], dmul(up[2], f.cu)));
+    vm = dadd(vm, dadd(up[1], dmul(up[2], f.cv)));
+    wm = dadd(wm, up[2]);
+  }
+  if (d.nrows > 1) {
+    const double dn = (double)d.nrows;
+    um = um / dn;
+    vm = vm / dn;
+    wm = wm / dn;
+  }
+  const double rw = (d.ch1 - d.ch0 == 1 && vs.recip_wvl) ? vs.recip_wvl[d.ch0] : d.freqmean / kC;
+  return block_geometry(f, um, vm, wm, rw, g);
+}
+
+// Stokes prediction -> correlations, Jones, smearing, phasor; subtract from the visibilities.
+template <int NPOL>
+__device__ __forceinline__ void degrid_block_apply(const ddfg_vis &vs, const ddfg_jones &js, const ddfg_facet &f,
+                                                   const DegridParams &dp, const DegridBlock &d, const float2 *pred) {
+  float2 s[4];
+#pragma unroll
+  for (int p = 0; p < 4; ++p) s[p] = (p < NPOL) ? pred[p] : czero();
+  M2 corr_vis = corr_from_stokes(dp.policy, s);
+  JonesCache jc;
+  jc.reset();
+  const int mid = d.rows[d.nrows / 2];
+  if (js.mode == 2) {
+    const double *up = vs.uvw + 3 * (int64_t)mid;
+    jc.update(js, f.idir_kms, f.idir_beam, mid, (d.ch0 + d.ch1) / 2, up[0], up[1]);
+    corr_vis = m2_times(m2_times(jc.j0, corr_vis), m2_herm(jc.j1));
+  }
+  const float dec = (float)decorr_factor(vs, f, d.freqmean, mid);
+  const double n0m1 = sqrt(1. - f.l0 * f.l0 - f.m0 * f.m0) - 1.;
+  const int nchan = vs.nchan, ncorr = vs.ncorr;
+  float2 *visd = (float2 *)vs.vis;
+  for (int inx = 0; inx < d.nrows; ++inx) {
+    const int64_t irow = d.rows[inx];
+    const double *up = vs.uvw + 3 * irow;
+    const double dot = up[0] * f.l0 + up[1] * f.m0 + up[2] * n0m1;
+    for (int ch = d.ch0; ch < d.ch1; ++ch) {
+      const float2 ph = cscale(phasor_turns(vs.freqs[ch] * dot * kInvC), dec);
+      M2 vb;
+      if (js.mode == 1) {
+        jc.update(js, f.idir_kms, f.idir_beam, irow, ch, up[0], up[1]);
+        vb = m2_scale(m2_times(m2_times(jc.j0, corr_vis), m2_herm(jc.j1)), ph);
+      } else {
+        vb = m2_scale(corr_vis, ph);
+      }
+      float2 *vp = visd + (irow * nchan + ch) * (int64_t)ncorr;
+      // subtractVis<nVisCorr> (degridder.h:43-53)
+      if (ncorr == 4) {
+        float4 a = *(float4 *)vp, c = *(float4 *)(vp + 2);
+        a.x -= vb.v[0].x; a.y -= vb.v[0].y; a.z -= vb.v[1].x; a.w -= vb.v[1].y;
+        c.x -= vb.v[2].x; c.y -= vb.v[2].y; c.z -= vb.v[3].x; c.w -= vb.v[3].y;
+        *(float4 *)vp = a;
+        *(float4 *)(vp + 2) = c;
+      } else if (ncorr == 2) {
+        vp[0] = csub(vp[0], vb.v[0]);
+        vp[1] = csub(vp[1], vb.v[3]);
+      } else {
+        vp[0] = csub(vp[0], vb.v[0]);
+      }
+    }
+  }
+}
+
+}  // namespace ddfg

@@ -19,196 +19,26 @@
 #include <cuda_runtime.h>
 
 #include "ddfg_common.cuh"
+#include "ddfg_gridblock.cuh"
 #include "ddfg_internal.h"
 
 namespace ddfg {
 
-struct FacetPack {
-  ddfg_facet f[DDFG_FACETS_PER_LAUNCH];
-  int n;
-};
-
-struct GridParams {
-  int policy;       // GridPolicy
-  int nvispol;      // Stokes products formed by the policy
-  int dopsf;
-  double freq_mean0;  // mean of all channel frequencies (gridder.h:164-171)
-};
-
-// Result of one lane's block walk.
-template <int NPOL>
-struct GridRecord {
-  bool valid;
-  int gridchan;
-  BlockGeom g;
-  float2 stokes[NPOL];
-  double weight;          // ThisWeight
-  double sumjones;        // ThisSumJones
-  double sumsqw;          // ThisSumSqWeights
-};
-
-// Walk one block for one facet: gridder.h:184-351.
-template <int NPOL>
-__device__ __forceinline__ void grid_block_record(const ddfg_vis &vs, const ddfg_jones &js, const ddfg_facet &f,
-                                                  const GridParams &gp, int64_t b, double n0m1,
-                                                  GridRecord<NPOL> &rec, JonesCache &jc) {
-  rec.valid = false;
-  if (vs.sparsification && !vs.sparsification[b]) return;
-  const int64_t start = vs.block_start[b];
-  const int nrows_blk = vs.bda_map[2 + b] - 2;
-  const int ch0 = vs.bda_map[start], ch1 = vs.bda_map[start + 1];
-  const int32_t *rows = vs.bda_map + start + 2;
-  const int nchan = vs.nchan, ncorr = vs.ncorr;
-  if (nrows_blk <= 0) return;  // no rows: the reference grids nothing either (gridder.h:283)
-
-  jc.reset();
-  const double dec = decorr_factor(vs, f, gp.freq_mean0, rows[nrows_blk / 2]);
-  const float decf = (float)dec;
-
-  M2 vis_acc;
-#pragma unroll
-  for (int p = 0; p < 4; ++p) vis_acc.v[p] = czero();
-  M2 vmeas;
-  vmeas.v[0] = make_float2(decf, 0.f);
-  vmeas.v[1] = czero();
-  vmeas.v[2] = czero();
-  vmeas.v[3] = make_float2(decf, 0.f);
-  bool have_psf = false;
-
-  double umean = 0., vmean = 0., wmean = 0., freqmean = 0., thisweight = 0., sumjones = 0., sumsqw = 0.;
-  double chanmean = 0.;
-  int nvis = 0;
-  const float2 *visd = (const float2 *)vs.vis;
-
-  for (int inx = 0; inx < nrows_blk; ++inx) {
-    const int64_t irow = rows[inx];
-    const double *up = vs.uvw + 3 * irow;
-    const double U = up[0], V = up[1], W = up[2];
-    // angle = -2 pi (U l0 + V m0 + W n0) / c  ->  phase in turns = -nu * dot / c
-    const double dot = U * f.l0 + V * f.m0 + W * n0m1;
-    for (int ch = ch0; ch < ch1; ++ch) {
-      const int64_t doff = (irow * nchan + ch) * (int64_t)ncorr;
-      if (vs.flags[doff]) continue;
-      const double nu = vs.freqs[ch];
-      const float2 corr = gp.dopsf ? make_float2(1.f, 0.f) : phasor_turns(-nu * dot / kC);
-      if (js.mode == 1) {
-        const bool chg = jc.update(js, f.idir_kms, f.idir_beam, irow, ch, U, V);
-        if ((chg || !have_psf) && gp.dopsf) {
-          vmeas = m2_times(jc.j0, jc.j1h);
-          vmeas = m2_times(m2_times(jc.j0h, vmeas), jc.j1);
-          vmeas = m2_scale(vmeas, make_float2(decf, 0.f));
-          have_psf = true;
-        }
-      }
-      if (!gp.dopsf) {
-        // Read_4Corr / Read_2Corr_Pad / Read_1Corr_Pad (gridder.h:44-60)
-        const float2 *vp = visd + doff;
-        if (ncorr == 4) {
-          vmeas.v[0] = vp[0]; vmeas.v[1] = vp[1]; vmeas.v[2] = vp[2]; vmeas.v[3] = vp[3];
-        } else if (ncorr == 2) {
-          vmeas.v[0] = vp[0]; vmeas.v[1] = czero(); vmeas.v[2] = czero(); vmeas.v[3] = vp[1];
-        } else {
-          vmeas.v[0] = vp[0]; vmeas.v[1] = czero(); vmeas.v[2] = czero(); vmeas.v[3] = vp[0];
-        }
-      }
-      const double fw = (double)vs.weights[irow * nchan + ch];  // * WeightVaryJJ (=1)
-      const float2 wgt = cscale(corr, (float)fw);
-      const double fwd = fw * dec * dec;
-      sumsqw += fwd;
-      if (js.mode == 1) {
-        if (!gp.dopsf) vmeas = m2_times(m2_times(jc.j0h, vmeas), jc.j1);
-        sumjones += (double)jc.bb * fwd;
-      }
-      // Mulaccum_{4Corr,2Corr_Unpad,1Corr_Unpad} (gridder.h:63-76)
-      vis_acc.v[0] = cadd(vis_acc.v[0], cmul(vmeas.v[0], wgt));
-      if (ncorr == 4) {
-        vis_acc.v[1] = cadd(vis_acc.v[1], cmul(vmeas.v[1], wgt));
-        vis_acc.v[2] = cadd(vis_acc.v[2], cmul(vmeas.v[2], wgt));
-      }
-      if (ncorr >= 2) vis_acc.v[3] = cadd(vis_acc.v[3], cmul(vmeas.v[3], wgt));
-      // Block means (gridder.h:272-279), FP64, uncontracted, reference order.
-      umean = dadd(umean, dadd(U, dmul(W, f.cu)));
-      vmean = dadd(vmean, dadd(V, dmul(W, f.cv)));
-      wmean = dadd(wmean, W);
-      freqmean = dadd(freqmean, nu);
-      thisweight += fw;
-      chanmean += (double)vs.chan_map[ch];
-      ++nvis;
-    }
-  }
-  if (nvis == 0) return;
-  const double dn = (double)nvis;
-  umean = umean / dn;
-  vmean = vmean / dn;
-  wmean = wmean / dn;
-  freqmean = freqmean / dn;
-  (void)chanmean;
-
-  if (js.mode == 2) {
-    // BDAJones: one Jones pair per block at the middle row / middle channel (gridder.h:291-301)
-    jc.reset();
-    jc.update(js, f.idir_kms, f.idir_beam, rows[nrows_blk / 2], (ch0 + ch1) / 2, umean, vmean);
-    if (gp.dopsf) vis_acc = m2_times(m2_times(jc.j0, vis_acc), jc.j1h);
-    vis_acc = m2_times(m2_times(jc.j0h, vis_acc), jc.j1);
-    sumjones = sumsqw * (double)jc.bb;
-  }
-  const int gridchan = vs.chan_map[ch0];
-  if (gridchan < 0 || gridchan >= f.nband) return;
-  const double recip_wvl = freqmean / kC;
-  if (!block_geometry(f, umean, vmean, wmean, recip_wvl, rec.g)) return;
-
-  float2 st[4];
-  stokes_from_corr(gp.policy, vis_acc, st);
-#pragma unroll
-  for (int p = 0; p < NPOL; ++p) rec.stokes[p] = st[p];
-  rec.valid = true;
-  rec.gridchan = gridchan;
-  rec.weight = thisweight;
-  rec.sumjones = sumjones;
-  rec.sumsqw = sumsqw;
-}
-
-// Second walk of a valid block for the per-channel Jones sums (gridder.h:254-263, 299-300,
-// 369-373), added straight into the CTA's shared accumulators.
-__device__ __forceinline__ void grid_block_chan_sums(const ddfg_vis &vs, const ddfg_jones &js, const ddfg_facet &f,
-                                                     const GridParams &gp, int64_t b, float block_bb, double mult,
-                                                     double *s_chan, JonesCache &jc) {
-  const int64_t start = vs.block_start[b];
-  const int nrows_blk = vs.bda_map[2 + b] - 2;
-  const int ch0 = vs.bda_map[start], ch1 = vs.bda_map[start + 1];
-  const int32_t *rows = vs.bda_map + start + 2;
-  const double dec = decorr_factor(vs, f, gp.freq_mean0, rows[nrows_blk / 2]);
-  const int nchan = vs.nchan;
-  jc.reset();
-  for (int inx = 0; inx < nrows_blk; ++inx) {
-    const int64_t irow = rows[inx];
-    const double *up = vs.uvw + 3 * irow;
-    for (int ch = ch0; ch < ch1; ++ch) {
-      const int64_t doff = (irow * nchan + ch) * (int64_t)vs.ncorr;
-      if (vs.flags[doff]) continue;
-      const double fwd = (double)vs.weights[irow * nchan + ch] * dec * dec;
-      double bbv = (double)block_bb;
-      if (js.mode == 1) {
-        jc.update(js, f.idir_kms, f.idir_beam, irow, ch, up[0], up[1]);
-        bbv = (double)jc.bb;
-      }
-      atomicAdd(&s_chan[ch], mult * bbv * fwd);
-      atomicAdd(&s_chan[nchan + ch], mult * fwd);
-    }
-  }
-}
-
 template <int NPOL>
 __global__ void __launch_bounds__(256) grid_kernel(const ddfg_vis vs, const ddfg_jones js, const FacetPack pack,
                                                    const GridParams gp) {
-  extern __shared__ double s_acc[];
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  ddfg_facet *sf = (ddfg_facet *)smem_raw;
+  double *s_acc = (double *)(sf + pack.n);
+  stage_facets(pack, sf);
   const int lane = threadIdx.x & 31;
   const int warp = threadIdx.x >> 5;
   const int nwarps = blockDim.x >> 5;
   const int64_t nstripes = (vs.nblocks + 31) / 32;
 
   for (int fi = 0; fi < pack.n; ++fi) {
-    const ddfg_facet &f = pack.f[fi];
+    __syncthreads();
+    const ddfg_facet &f = sf[fi];
     const int npol_used = min(gp.nvispol, f.npol);
     const int nsw = f.nband * f.npol;
     double *s_sumwt = s_acc;                  // [nband][npol]
@@ -229,16 +59,7 @@ __global__ void __launch_bounds__(256) grid_kernel(const ddfg_vis vs, const ddfg
       rec.valid = false;
       if (b < vs.nblocks) grid_block_record<NPOL>(vs, js, f, gp, b, n0m1, rec, jc);
 
-      if (rec.valid) {
-        for (int p = 0; p < npol_used; ++p) atomicAdd(&s_sumwt[rec.gridchan * f.npol + p], rec.weight);
-        if (js.mode != 0) {
-          const double m = (double)npol_used;
-          atomicAdd(&s_sumj[rec.gridchan], m * rec.sumjones);
-          atomicAdd(&s_sumj[f.nband + rec.gridchan], m * rec.sumsqw);
-          const float block_bb = jc.bb;  // the block's Jones after a BDAJones walk
-          grid_block_chan_sums(vs, js, f, gp, b, block_bb, m, s_chan, jc);
-        }
-      }
+      warp_add_block_sums<NPOL>(vs, js, f, gp, b, rec, npol_used, s_sumwt, s_sumj, s_chan, jc);
 
       // Warp-cooperative tap scatter of the 32 records (gridder.h:353-362).
       unsigned mask = __ballot_sync(0xffffffffu, rec.valid);
@@ -248,6 +69,7 @@ __global__ void __launch_bounds__(256) grid_kernel(const ddfg_vis vs, const ddfg
         const int locx = __shfl_sync(0xffffffffu, rec.g.locx, src);
         const int locy = __shfl_sync(0xffffffffu, rec.g.locy, src);
         const int S = __shfl_sync(0xffffffffu, rec.g.S, src);
+        const unsigned inv = __shfl_sync(0xffffffffu, rec.g.inv, src);
         const int gch = __shfl_sync(0xffffffffu, rec.gridchan, src);
         const float2 *cf = (const float2 *)__shfl_sync(0xffffffffu, (unsigned long long)rec.g.cf, src);
         float2 sv[NPOL];
@@ -258,7 +80,6 @@ __global__ void __launch_bounds__(256) grid_kernel(const ddfg_vis vs, const ddfg
         }
         const int sup = (S - 1) >> 1;
         const int ntap = S * S;
-        const unsigned inv = (65536u + (unsigned)S - 1u) / (unsigned)S;  // exact t/S for t < S*S, S <= 63
         float2 *g0 = grid + (size_t)gch * f.npol * plane_sz + (size_t)(locy - sup) * f.nx + (locx - sup);
         for (int t = lane; t < ntap; t += 32) {
           const int sy = (int)(((unsigned)t * inv) >> 16);
@@ -299,7 +120,7 @@ int ddfg_launch_grid(const ddfg_vis *vs, const ddfg_jones *js, const ddfg_facet 
   gp.freq_mean0 = vs->freq_mean;
   int max_band = 1;
   for (int i = 0; i < nfacets; ++i) max_band = max(max_band, facets[i].nband * (facets[i].npol + 2));
-  const size_t smem = sizeof(double) * ((size_t)max_band + 2 * (size_t)vs->nchan);
+  const size_t smem = sizeof(ddfg_facet) * DDFG_FACETS_PER_LAUNCH + sizeof(double) * ((size_t)max_band + 2 * (size_t)vs->nchan);
   if (smem > 160 * 1024) return ddfg_set_error(DDFG_ESIZE, "grid: too many bands/channels for the shared accumulators");
   for (int f0 = 0; f0 < nfacets; f0 += DDFG_FACETS_PER_LAUNCH) {
     FacetPack pack;

@@ -1,0 +1,244 @@
+// The gridder's per-block walk (shared by the direct and the tile-sorted gridding kernels).
+#pragma once
+#include "ddfg_common.cuh"
+
+namespace ddfg {
+
+struct FacetPack {
+  ddfg_facet f[DDFG_FACETS_PER_LAUNCH];
+  int n;
+};
+
+struct GridParams {
+  int policy;       // GridPolicy
+  int nvispol;      // Stokes products formed by the policy
+  int dopsf;
+  double freq_mean0;  // mean of all channel frequencies (gridder.h:164-171)
+};
+
+// Result of one lane's block walk.
+template <int NPOL>
+struct GridRecord {
+  bool valid;
+  int gridchan;
+  BlockGeom g;
+  float2 stokes[NPOL];
+  double weight;          // ThisWeight
+  double sumjones;        // ThisSumJones
+  double sumsqw;          // ThisSumSqWeights
+  int ch0;                // first channel of the block
+  bool single_chan;       // one channel: its channel sums are the block sums
+};
+
+// Walk one block for one facet: gridder.h:184-351.
+template <int NPOL>
+__device__ __forceinline__ void grid_block_record(const ddfg_vis &vs, const ddfg_jones &js, const ddfg_facet &f,
+                                                  const GridParams &gp, int64_t b, double n0m1,
+                                                  GridRecord<NPOL> &rec, JonesCache &jc) {
+  rec.valid = false;
+  if (vs.sparsification && !vs.sparsification[b]) return;
+  const int64_t start = vs.block_start[b];
+  const int nrows_blk = vs.bda_map[2 + b] - 2;
+  const int ch0 = vs.bda_map[start], ch1 = vs.bda_map[start + 1];
+  const int32_t *rows = vs.bda_map + start + 2;
+  const int nchan = vs.nchan, ncorr = vs.ncorr;
+  if (nrows_blk <= 0) return;  // no rows: the reference grids nothing either (gridder.h:283)
+
+  jc.reset();
+  const double dec = decorr_factor(vs, f, gp.freq_mean0, rows[nrows_blk / 2]);
+  const float decf = (float)dec;
+
+  M2 vis_acc;
+#pragma unroll
+  for (int p = 0; p < 4; ++p) vis_acc.v[p] = czero();
+  M2 vmeas;
+  vmeas.v[0] = make_float2(decf, 0.f);
+  vmeas.v[1] = czero();
+  vmeas.v[2] = czero();
+  vmeas.v[3] = make_float2(decf, 0.f);
+  bool have_psf = false;
+
+  double umean = 0., vmean = 0., wmean = 0., freqmean = 0., thisweight = 0., sumjones = 0., sumsqw = 0.;
+  int nvis = 0, last_ch = ch0;
+  const float2 *visd = (const float2 *)vs.vis;
+
+  for (int inx = 0; inx < nrows_blk; ++inx) {
+    const int64_t irow = rows[inx];
+    const double *up = vs.uvw + 3 * irow;
+    const double U = up[0], V = up[1], W = up[2];
+    // angle = -2 pi (U l0 + V m0 + W n0) / c  ->  phase in turns = -nu * dot / c
+    const double dot = U * f.l0 + V * f.m0 + W * n0m1;
+    for (int ch = ch0; ch < ch1; ++ch) {
+      const int64_t doff = (irow * nchan + ch) * (int64_t)ncorr;
+      if (vs.flags[doff]) continue;
+      const double nu = vs.freqs[ch];
+      const float2 corr = gp.dopsf ? make_float2(1.f, 0.f) : phasor_turns(-nu * dot * kInvC);
+      if (js.mode == 1) {
+        const bool chg = jc.update(js, f.idir_kms, f.idir_beam, irow, ch, U, V);
+        if ((chg || !have_psf) && gp.dopsf) {
+          vmeas = m2_times(jc.j0, m2_herm(jc.j1));
+          vmeas = m2_times(m2_times(m2_herm(jc.j0), vmeas), jc.j1);
+          vmeas = m2_scale(vmeas, make_float2(decf, 0.f));
+          have_psf = true;
+        }
+      }
+      if (!gp.dopsf) {
+        // Read_4Corr / Read_2Corr_Pad / Read_1Corr_Pad (gridder.h:44-60)
+        const float2 *vp = visd + doff;
+        if (ncorr == 4) {
+          vmeas.v[0] = vp[0]; vmeas.v[1] = vp[1]; vmeas.v[2] = vp[2]; vmeas.v[3] = vp[3];
+        } else if (ncorr == 2) {
+          vmeas.v[0] = vp[0]; vmeas.v[1] = czero(); vmeas.v[2] = czero(); vmeas.v[3] = vp[1];
+        } else {
+          vmeas.v[0] = vp[0]; vmeas.v[1] = czero(); vmeas.v[2] = czero(); vmeas.v[3] = vp[0];
+        }
+      }
+      const double fw = (double)vs.weights[irow * nchan + ch];  // * WeightVaryJJ (=1)
+      const float2 wgt = cscale(corr, (float)fw);
+      const double fwd = fw * dec * dec;
+      sumsqw += fwd;
+      if (js.mode == 1) {
+        if (!gp.dopsf) vmeas = m2_times(m2_times(m2_herm(jc.j0), vmeas), jc.j1);
+        sumjones += (double)jc.bb * fwd;
+      }
+      // Mulaccum_{4Corr,2Corr_Unpad,1Corr_Unpad} (gridder.h:63-76)
+      vis_acc.v[0] = cadd(vis_acc.v[0], cmul(vmeas.v[0], wgt));
+      if (ncorr == 4) {
+        vis_acc.v[1] = cadd(vis_acc.v[1], cmul(vmeas.v[1], wgt));
+        vis_acc.v[2] = cadd(vis_acc.v[2], cmul(vmeas.v[2], wgt));
+      }
+      if (ncorr >= 2) vis_acc.v[3] = cadd(vis_acc.v[3], cmul(vmeas.v[3], wgt));
+      // Block means (gridder.h:272-279), FP64, uncontracted, reference order.
+      umean = dadd(umean, dadd(U, dmul(W, f.cu)));
+      vmean = dadd(vmean, dadd(V, dmul(W, f.cv)));
+      wmean = dadd(wmean, W);
+      freqmean = dadd(freqmean, nu);
+      thisweight += fw;
+      last_ch = ch;
+      ++nvis;
+    }
+  }
+  if (nvis == 0) return;
+  if (nvis > 1) {  // x / 1.0 == x exactly, so single-visibility blocks skip the divisions
+    const double dn = (double)nvis;
+    umean = umean / dn;
+    vmean = vmean / dn;
+    wmean = wmean / dn;
+    freqmean = freqmean / dn;
+  }
+
+  if (js.mode == 2) {
+    // BDAJones: one Jones pair per block at the middle row / middle channel (gridder.h:291-301)
+    jc.reset();
+    jc.update(js, f.idir_kms, f.idir_beam, rows[nrows_blk / 2], (ch0 + ch1) / 2, umean, vmean);
+    if (gp.dopsf) vis_acc = m2_times(m2_times(jc.j0, vis_acc), m2_herm(jc.j1));
+    vis_acc = m2_times(m2_times(m2_herm(jc.j0), vis_acc), jc.j1);
+    sumjones = sumsqw * (double)jc.bb;
+  }
+  const int gridchan = vs.chan_map[ch0];
+  if (gridchan < 0 || gridchan >= f.nband) return;
+  // FreqMean / C; a single-visibility block's mean is its channel frequency, whose quotient
+  // the host tabulated with the same IEEE division.
+  const double recip_wvl = (nvis == 1 && vs.recip_wvl) ? vs.recip_wvl[last_ch] : freqmean / kC;
+  if (!block_geometry(f, umean, vmean, wmean, recip_wvl, rec.g)) return;
+
+  float2 st[4];
+  stokes_from_corr(gp.policy, vis_acc, st);
+#pragma unroll
+  for (int p = 0; p < NPOL; ++p) rec.stokes[p] = st[p];
+  rec.valid = true;
+  rec.gridchan = gridchan;
+  rec.weight = thisweight;
+  rec.sumjones = sumjones;
+  rec.sumsqw = sumsqw;
+  rec.ch0 = ch0;
+  rec.single_chan = (ch1 - ch0 == 1);
+}
+
+// Per-channel Jones sums of a valid block (gridder.h:254-263, 299-300, 369-373) into the CTA's
+// shared accumulators: the block sums for a single-channel block, else a second walk.
+template <int NPOL>
+__device__ __forceinline__ void grid_block_add_chan_sums(const ddfg_vis &vs, const ddfg_jones &js,
+                                                         const ddfg_facet &f, const GridParams &gp, int64_t b,
+                                                         const GridRecord<NPOL> &rec, double mult, double *s_chan,
+                                                         JonesCache &jc);
+
+// Second walk of a valid block for the per-channel Jones sums.
+__device__ __forceinline__ void grid_block_chan_sums(const ddfg_vis &vs, const ddfg_jones &js, const ddfg_facet &f,
+                                                     const GridParams &gp, int64_t b, float block_bb, double mult,
+                                                     double *s_chan, JonesCache &jc) {
+  const int64_t start = vs.block_start[b];
+  const int nrows_blk = vs.bda_map[2 + b] - 2;
+  const int ch0 = vs.bda_map[start], ch1 = vs.bda_map[start + 1];
+  const int32_t *rows = vs.bda_map + start + 2;
+  const double dec = decorr_factor(vs, f, gp.freq_mean0, rows[nrows_blk / 2]);
+  const int nchan = vs.nchan;
+  jc.reset();
+  for (int inx = 0; inx < nrows_blk; ++inx) {
+    const int64_t irow = rows[inx];
+    const double *up = vs.uvw + 3 * irow;
+    for (int ch = ch0; ch < ch1; ++ch) {
+      const int64_t doff = (irow * nchan + ch) * (int64_t)vs.ncorr;
+      if (vs.flags[doff]) continue;
+      const double fwd = (double)vs.weights[irow * nchan + ch] * dec * dec;
+      double bbv = (double)block_bb;
+      if (js.mode == 1) {
+        jc.update(js, f.idir_kms, f.idir_beam, irow, ch, up[0], up[1]);
+        bbv = (double)jc.bb;
+      }
+      atomicAdd(&s_chan[ch], mult * bbv * fwd);
+      atomicAdd(&s_chan[nchan + ch], mult * fwd);
+    }
+  }
+}
+
+template <int NPOL>
+__device__ __forceinline__ void grid_block_add_chan_sums(const ddfg_vis &vs, const ddfg_jones &js,
+                                                         const ddfg_facet &f, const GridParams &gp, int64_t b,
+                                                         const GridRecord<NPOL> &rec, double mult, double *s_chan,
+                                                         JonesCache &jc) {
+  if (rec.single_chan) {
+    atomicAdd(&s_chan[rec.ch0], mult * rec.sumjones);
+    atomicAdd(&s_chan[vs.nchan + rec.ch0], mult * rec.sumsqw);
+  } else {
+    const float block_bb = jc.bb;
+    grid_block_chan_sums(vs, js, f, gp, b, block_bb, mult, s_chan, jc);
+  }
+}
+
+// The warp's 32 records' contributions to the weight and Jones sums (gridder.h:363-373): one
+// shared-memory update per warp when every valid lane grids into the same band, per lane
+// otherwise.  Must be called by all 32 lanes.
+template <int NPOL>
+__device__ __forceinline__ void warp_add_block_sums(const ddfg_vis &vs, const ddfg_jones &js, const ddfg_facet &f,
+                                                    const GridParams &gp, int64_t b, const GridRecord<NPOL> &rec,
+                                                    int npol_used, double *a_sumwt, double *a_sumj, double *a_chan,
+                                                    JonesCache &jc) {
+  const unsigned vmask = __ballot_sync(0xffffffffu, rec.valid);
+  if (!vmask) return;
+  const int lane = threadIdx.x & 31;
+  const int g0 = __shfl_sync(0xffffffffu, rec.gridchan, __ffs(vmask) - 1);
+  const bool same = __all_sync(0xffffffffu, !rec.valid || rec.gridchan == g0);
+  double wsum = rec.valid ? rec.weight : 0., jsum = rec.valid ? rec.sumjones : 0., qsum = rec.valid ? rec.sumsqw : 0.;
+  if (same) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      wsum += __shfl_xor_sync(0xffffffffu, wsum, o);
+      if (js.mode != 0) {
+        jsum += __shfl_xor_sync(0xffffffffu, jsum, o);
+        qsum += __shfl_xor_sync(0xffffffffu, qsum, o);
+      }
+    }
+  }
+  if ((same && lane == 0) || (!same && rec.valid)) {
+    const int g = same ? g0 : rec.gridchan;
+    for (int p = 0; p < npol_used; ++p) atomicAdd(&a_sumwt[g * f.npol + p], wsum);
+    if (js.mode != 0) {
+      atomicAdd(&a_sumj[g], (double)npol_used * jsum);
+      atomicAdd(&a_sumj[f.nband + g], (double)npol_used * qsum);
+    }
+  }
+  if (js.mode != 0 && rec.valid) grid_block_add_chan_sums<NPOL>(vs, js, f, gp, b, rec, (double)npol_used, a_chan, jc);
+}
+
+}  // namespace ddfg

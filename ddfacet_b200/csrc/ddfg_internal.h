@@ -2,7 +2,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
-#include "../../include/ddfg.h"
+#include "ddfg.h"
 
 // Records the message of the failing call for ddfg_last_error() and returns code.
 int ddfg_set_error(int code, const char *fmt, ...);
@@ -13,3 +13,9 @@ int ddfg_launch_grid(const ddfg_vis *vs, const ddfg_jones *js, const ddfg_facet 
                      int nvispol, int dopsf, int num_ctas, cudaStream_t stream);
 int ddfg_launch_degrid(const ddfg_vis *vs, const ddfg_jones *js, const ddfg_facet *facets, int nfacets, int policy,
                        int nvispol, int num_ctas, cudaStream_t stream);
+int ddfg_launch_grid_sorted(const ddfg_vis *vs, const ddfg_jones *js, const ddfg_facet *facets, int nfacets, int policy,
+                            int nvispol, int dopsf, const ddfg_sort_plan *plan, int compensated, int max_support,
+                            int facets_per_launch, cudaStream_t stream);
+int ddfg_launch_degrid_sorted(const ddfg_vis *vs, const ddfg_jones *js, const ddfg_facet *facets, int nfacets,
+                              int policy, int nvispol, const ddfg_sort_plan *plan, int max_support,
+                              int facets_per_launch, cudaStream_t stream);

@@ -65,6 +65,7 @@ class VisData:
     weights: torch.Tensor        # float32 [nrow, nchan]
     freqs: torch.Tensor          # float64 [nchan]
     freqs_host: np.ndarray
+    recip_wvl: torch.Tensor      # float64 [nchan] freqs / c (the IEEE quotient the reference forms)
     chan_map: torch.Tensor       # int32 [nchan]
     bda_map: torch.Tensor        # int32
     block_start: torch.Tensor    # int64 [nblocks]
@@ -126,6 +127,7 @@ class VisData:
             weights=to_device(weights, torch.float32, device, non_blocking=non_blocking),
             freqs=to_device(freqs_host, torch.float64, device),
             freqs_host=freqs_host,
+            recip_wvl=to_device(freqs_host / C_LIGHT, torch.float64, device),
             chan_map=to_device(np.asarray(chan_map, np.int32) if not isinstance(chan_map, torch.Tensor) else chan_map,
                                torch.int32, device),
             bda_map=bm,
@@ -149,6 +151,7 @@ class VisData:
         s.weights = self.weights.data_ptr()
         s.freqs = self.freqs.data_ptr()
         s.freq_mean = float(np.mean(self.freqs_host)) if self.freqs_host.size else 0.0
+        s.recip_wvl = self.recip_wvl.data_ptr()
         s.chan_map = self.chan_map.data_ptr()
         s.nrow, s.nchan, s.ncorr = nrow, nchan, ncorr
         s.chan_equidistant = self.chan_equidistant
@@ -173,6 +176,7 @@ class CFTables:
     overs: int
     ref_wave: float
     wmax: float
+    max_support: int = 0
 
     @classmethod
     def create(cls, wplanes: Sequence[np.ndarray], wplanes_conj: Sequence[np.ndarray], overs: int, ref_wave: float,
@@ -190,7 +194,7 @@ class CFTables:
             raise ValueError("W planes and their conjugates must have the same supports")
         return cls(data=to_device(packed, torch.complex64, device), off_grid=to_device(offs, torch.int64, device),
                    off_degrid=to_device(off_d, torch.int64, device), sup=to_device(sup, torch.int32, device), nw=nw,
-                   overs=int(overs), ref_wave=float(ref_wave), wmax=float(wmax))
+                   overs=int(overs), ref_wave=float(ref_wave), wmax=float(wmax), max_support=int(sup.max()))
 
 
 @dataclass
@@ -220,6 +224,7 @@ class FacetGrid:
         s.cf_offset = (self.cf.off_degrid if degrid else self.cf.off_grid).data_ptr()
         s.cf_support = self.cf.sup.data_ptr()
         s.nw, s.overs = self.cf.nw, self.cf.overs
+        s.max_support = int(self.cf.max_support)
         s.ref_wave, s.wmax = self.cf.ref_wave, self.cf.wmax
         s.idir_kms, s.idir_beam = int(self.idir_kms), int(self.idir_beam)
         s.decorr_l, s.decorr_m = float(self.decorr_lm[0]), float(self.decorr_lm[1])
@@ -302,3 +307,50 @@ def degrid(vs: VisData, facets: List[FacetGrid], pol: _abi.Pol, jones: Optional[
     js = (jones or JonesData()).struct()
     vss = vs.struct()
     _abi.check(lib.ddfg_degrid(C.byref(vss), C.byref(js), C.byref(pol), arr, len(facets), _stream_ptr(stream)))
+
+
+@dataclass
+class SortPlan:
+    """Work list of the batched kernels (ddfg_sort_plan_build): block indices sorted by (band,
+    W-plane support, grid row, grid column) on the largest facet grid."""
+    perm: torch.Tensor
+    st: _abi.SortPlan
+
+    @classmethod
+    def build(cls, vs: VisData, facets: List[FacetGrid], chunk=1024, stream=None):
+        lib = _abi.lib()
+        ref = max(facets, key=lambda f: f.grid.shape[-1])
+        nb = vs.nblocks
+        perm = torch.empty(max(nb, 1), dtype=torch.int64, device=vs.vis.device)
+        p = _abi.SortPlan()
+        p.perm = perm.data_ptr()
+        p.chunk = int(chunk)
+        ws = torch.empty(int(lib.ddfg_sort_plan_workspace_size(nb)), dtype=torch.uint8, device=vs.vis.device)
+        vss = vs.struct()
+        fs = ref.struct()
+        _abi.check(lib.ddfg_sort_plan_build(C.byref(vss), C.byref(fs), C.byref(p), ws.data_ptr(), ws.numel(),
+                                            _stream_ptr(stream)))
+        return cls(perm, p)
+
+
+def grid_sorted(vs: VisData, facets: List[FacetGrid], pol: _abi.Pol, plan: SortPlan, jones: Optional[JonesData] = None,
+                dopsf=False, compensated=True, facets_per_launch=0, stream=None):
+    """Grid ``vs`` onto every facet through the sort plan (ddfg_grid_sorted)."""
+    lib = _abi.lib()
+    arr = (_abi.Facet * max(1, len(facets)))(*[f.struct(degrid=False) for f in facets])
+    js = (jones or JonesData()).struct()
+    vss = vs.struct()
+    _abi.check(lib.ddfg_grid_sorted(C.byref(vss), C.byref(js), C.byref(pol), arr, len(facets), int(bool(dopsf)),
+                                    C.byref(plan.st), int(bool(compensated)), int(facets_per_launch),
+                                    _stream_ptr(stream)))
+
+
+def degrid_sorted(vs: VisData, facets: List[FacetGrid], pol: _abi.Pol, plan: SortPlan,
+                  jones: Optional[JonesData] = None, facets_per_launch=0, stream=None):
+    """Subtract every facet's prediction from ``vs.vis`` through the sort plan (ddfg_degrid_sorted)."""
+    lib = _abi.lib()
+    arr = (_abi.Facet * max(1, len(facets)))(*[f.struct(degrid=True) for f in facets])
+    js = (jones or JonesData()).struct()
+    vss = vs.struct()
+    _abi.check(lib.ddfg_degrid_sorted(C.byref(vss), C.byref(js), C.byref(pol), arr, len(facets), C.byref(plan.st),
+                                      int(facets_per_launch), _stream_ptr(stream)))

@@ -56,6 +56,7 @@ typedef struct ddfg_facet {
   const int64_t *cf_offset;    /* [2*nw] */
   const int32_t *cf_support;   /* [2*nw] */
   int32_t nw, overs;
+  int32_t max_support;         /* largest cf_support[] value (host copy)                  */
   double ref_wave, wmax;       /* WInfos[0], WInfos[1]                                    */
   int32_t idir_kms, idir_beam; /* Jones direction of this facet (LJones[6][0], [8][0])    */
   double decorr_l, decorr_m;   /* LSmearing[5..6]: lm at which smearing is evaluated      */
@@ -73,6 +74,7 @@ typedef struct ddfg_vis {
   const float *weights;        /* [nrow][nchan]                                           */
   const double *freqs;         /* [nchan] Hz                                              */
   double freq_mean;            /* mean of freqs[] (host value; gridder.h:164-171)         */
+  const double *recip_wvl;     /* [nchan] freqs[c] / 299792458 computed on the host, or NULL */
   const int32_t *chan_map;     /* [nchan] visibility channel -> grid band                 */
   int64_t nrow;
   int32_t nchan, ncorr;
@@ -115,6 +117,16 @@ typedef struct ddfg_pol {
   int32_t stokes_ids[4];
 } ddfg_pol;
 
+/* The work list of the batched kernels: blocks sorted by (grid band, support of the W plane,
+ * grid row, grid column) of their mean position on a reference facet grid.  Consecutive blocks
+ * then share grid cells, which the kernels exploit.  The caller owns perm. */
+typedef struct ddfg_sort_plan {
+  int64_t *perm;               /* [nblocks] block indices in sorted order                 */
+  int32_t chunk;               /* in: blocks per warp work item                           */
+  int32_t gref;                /* out: side of the reference facet grid                   */
+  int64_t nplanned;            /* out: blocks that can be gridded (sorted first)          */
+} ddfg_sort_plan;
+
 /* Library and device checks. */
 int ddfg_version(void);
 int ddfg_last_error(char *buf, int len);
@@ -146,6 +158,30 @@ int ddfg_grid(const ddfg_vis *vs, const ddfg_jones *js, const ddfg_pol *pol,
  * facet of a call is applied by the warp that owns the block, so the result is deterministic. */
 int ddfg_degrid(const ddfg_vis *vs, const ddfg_jones *js, const ddfg_pol *pol,
                 const ddfg_facet *facets, int nfacets, void *stream);
+
+/* Device scratch of ddfg_sort_plan_build (bytes). */
+size_t ddfg_sort_plan_workspace_size(int64_t nblocks);
+
+/* Keys every block of vs by its band, W-plane support and grid cell on the reference facet ref,
+ * and sorts the blocks (stable radix sort, so the order is deterministic).  A plan call: it
+ * synchronises the stream.  The plan stays valid while the block map, uvw, frequencies and
+ * channel map are unchanged; it does not depend on the visibilities, weights, flags or Jones. */
+int ddfg_sort_plan_build(const ddfg_vis *vs, const ddfg_facet *ref, ddfg_sort_plan *plan, void *workspace,
+                         size_t workspace_bytes, void *stream);
+
+/* ddfg_grid over a sort plan (the batched gridder).  Each warp walks a chunk of consecutive
+ * sorted blocks and keeps the footprint's tap sums in registers while the grid cell and support
+ * stay the same, writing them to the grid once per run; compensated != 0 adds TwoSum error terms
+ * to the register sums.  facets_per_launch (<= DDFG_FACETS_PER_LAUNCH, 0 = default) bounds the
+ * facets whose grids are live in L2 at once.  Facets of one call must share nband and npol. */
+int ddfg_grid_sorted(const ddfg_vis *vs, const ddfg_jones *js, const ddfg_pol *pol, const ddfg_facet *facets,
+                     int nfacets, int dopsf, const ddfg_sort_plan *plan, int compensated, int facets_per_launch,
+                     void *stream);
+
+/* ddfg_degrid over a sort plan (the batched degridder): each warp keeps the footprint's model
+ * grid values in registers while consecutive blocks share the grid cell. */
+int ddfg_degrid_sorted(const ddfg_vis *vs, const ddfg_jones *js, const ddfg_pol *pol, const ddfg_facet *facets,
+                       int nfacets, const ddfg_sort_plan *plan, int facets_per_launch, void *stream);
 
 #ifdef __cplusplus
 }

@@ -164,13 +164,17 @@ def _gpu_objs(c, model_grid=None, vis=None):
     return vs, fg, jd
 
 
-def run_gpu_grid(c, dopsf=False):
+def run_gpu_grid(c, dopsf=False, sorted_=False, compensated=True, chunk=256):
     import torch
 
     from ddfacet_b200 import device as D
 
     vs, fg, jd = _gpu_objs(c)
-    D.grid(vs, [fg], D.make_pol(c.corr_ids, c.stokes_ids), jd, dopsf=dopsf)
+    if sorted_:
+        plan = D.SortPlan.build(vs, [fg], chunk=chunk)
+        D.grid_sorted(vs, [fg], D.make_pol(c.corr_ids, c.stokes_ids), plan, jd, dopsf=dopsf, compensated=compensated)
+    else:
+        D.grid(vs, [fg], D.make_pol(c.corr_ids, c.stokes_ids), jd, dopsf=dopsf)
     torch.cuda.synchronize()
     out = {"grid": fg.grid.cpu().numpy(), "sumwt": fg.sumwt.cpu().numpy()}
     if c.jones:
@@ -179,14 +183,18 @@ def run_gpu_grid(c, dopsf=False):
     return out
 
 
-def run_gpu_degrid(c, model_grid, vis0=None):
+def run_gpu_degrid(c, model_grid, vis0=None, sorted_=False, chunk=256):
     import torch
 
     from ddfacet_b200 import device as D
 
     vis = np.zeros_like(c.vis) if vis0 is None else vis0.copy()
     vs, fg, jd = _gpu_objs(c, model_grid=model_grid, vis=vis)
-    D.degrid(vs, [fg], D.make_pol(c.corr_ids, c.stokes_ids), jd)
+    if sorted_:
+        plan = D.SortPlan.build(vs, [fg], chunk=chunk)
+        D.degrid_sorted(vs, [fg], D.make_pol(c.corr_ids, c.stokes_ids), plan, jd)
+    else:
+        D.degrid(vs, [fg], D.make_pol(c.corr_ids, c.stokes_ids), jd)
     torch.cuda.synchronize()
     return vs.vis.cpu().numpy()
 
