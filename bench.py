@@ -217,22 +217,18 @@ def run_gpu(args):
     w = configs.multifacet_dde(device=dev, scale=args.scale)
     torch.cuda.synchronize()
     t_build = time.perf_counter() - t_build
-    t_plan = time.perf_counter()
-    plan = D.SortPlan.build(w.vs, w.facets_grid, chunk=args.chunk)
-    torch.cuda.synchronize()
-    t_plan = time.perf_counter() - t_plan
     stream = torch.cuda.current_stream()
-    fpl = args.facets_per_launch
+    fpl = 16
 
     def step(ev=None):
         for f in w.facets_grid:
             f.grid.zero_()
         if ev:
             ev[0].record(stream)
-        D.degrid_sorted(w.vs, w.facets_model, w.pol, plan, w.jones, facets_per_launch=fpl)
+        D.degrid(w.vs, w.facets_model, w.pol, w.jones)
         if ev:
             ev[1].record(stream)
-        D.grid_sorted(w.vs, w.facets_grid, w.pol, plan, w.jones, facets_per_launch=fpl)
+        D.grid(w.vs, w.facets_grid, w.pol, w.jones)
         if ev:
             ev[2].record(stream)
 
@@ -372,10 +368,9 @@ def run_gpu(args):
         "kernels_ms": {"degrid_call": round(degrid_ms, 3), "grid_call": round(grid_ms, 3)},
         "plain": (None if plain_ms is None else
                   {"ms_per_step": round(plain_ms, 1), "value": round(world * nvis / (plain_ms * 1e-3) / 1e6, 3),
-                   "what": "direct kernels, blocks in map order, one facet per launch, global atomics",
+                   "what": "the same kernels, one facet per call (one launch per facet and direction)",
                    "batched_speedup": round(plain_ms / ms_step, 2)}),
-        "plan": {"blocks": int(plan.st.nplanned), "chunk": args.chunk, "build_s": round(t_plan, 2),
-                 "facets_per_launch": fpl},
+        "facets_per_launch": fpl,
         "roofline": {
             "bound": "hbm", "kernel": dom, "achieved": round(achieved, 2), "peak": hbm_peak, "unit": "GB/s",
             "frac": round(achieved / hbm_peak, 5), "peak_kind": peak_kind, "traffic": None,
@@ -436,8 +431,7 @@ def main():
     ap.add_argument("--scale", type=float, default=1.0)
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
     ap.add_argument("--plain", action="store_true", help="also time the one-facet-per-launch direct path")
-    ap.add_argument("--chunk", type=int, default=1024)
-    ap.add_argument("--facets-per-launch", dest="facets_per_launch", type=int, default=8)
+
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

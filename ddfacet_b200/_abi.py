@@ -51,6 +51,7 @@ class VisSet(C.Structure):
         ("chan_map", _vp),
         ("nrow", _i64), ("nchan", _i32), ("ncorr", _i32),
         ("chan_equidistant", _i32),
+        ("single_vis_blocks", _i32),
         ("bda_map", _vp), ("bda_len", _i64), ("block_start", _vp), ("nblocks", _i64),
         ("sparsification", _vp),
         ("uvw_dt", _vp), ("dt", _f64), ("dnu", _f64), ("do_tsmear", _i32), ("do_fsmear", _i32),
@@ -82,7 +83,8 @@ SIGNATURES = {
     "ddfg_version": (C.c_int, []),
     "ddfg_last_error": (C.c_int, [C.c_char_p, C.c_int]),
     "ddfg_bda_plan_workspace_size": (C.c_size_t, [_i64]),
-    "ddfg_bda_plan": (C.c_int, [_vp, _i64, _i64, _i64, _i32, _vp, _vp, C.c_size_t, _vp]),
+    "ddfg_bda_plan": (C.c_int, [_vp, _i64, _i64, _i64, _i32, _vp, _vp, C.c_size_t, _vp, C.POINTER(_i32)]),
+    "ddfg_bda_plan_noalloc": (C.c_int, [_vp, _i64, _i64, _i64, _i32, _vp, _vp, C.POINTER(_i32)]),
     "ddfg_grid": (C.c_int, [C.POINTER(VisSet), C.POINTER(Jones), C.POINTER(Pol), C.POINTER(Facet), C.c_int,
                             C.c_int, _vp]),
     "ddfg_degrid": (C.c_int, [C.POINTER(VisSet), C.POINTER(Jones), C.POINTER(Pol), C.POINTER(Facet), C.c_int,

@@ -203,8 +203,8 @@ struct JonesCache {
                            js.interp_mode);
         norm_jones(k0, js, uk, vk);
         norm_jones(k1, js, uk, vk);
-        a = m2_times(k0, a);
-        b = m2_times(k1, b);
+        a = js.beam ? m2_times(k0, a) : k0;
+        b = js.beam ? m2_times(k1, b) : k1;
       }
       j0 = a;
       j1 = b;
@@ -214,6 +214,33 @@ struct JonesCache {
     return changed;
   }
 };
+
+// J0, J1 and BB of one visibility without a cache: what JonesCache::update computes after a
+// reset (every single-visibility block resets the reference's cache, gridder.h:184).
+__device__ __forceinline__ void jones_pair(const ddfg_jones &js, int idir_kms, int idir_beam, int64_t irow, int ichan,
+                                           double u, double v, M2 &j0, M2 &j1, float &bb) {
+  const int a0 = js.a0[irow], a1 = js.a1[irow];
+  M2 a = m2_unity(), b = m2_unity();
+  if (js.beam) {
+    const int t = js.beam_tmap[irow], c = js.beam_cmap[ichan];
+    a = give_jones((const float2 *)js.beam, js.beam_dims, js.interp_coefs, t, a0, idir_beam, c, js.interp_mode);
+    b = give_jones((const float2 *)js.beam, js.beam_dims, js.interp_coefs, t, a1, idir_beam, c, js.interp_mode);
+  }
+  if (js.kms) {
+    const int t = js.kms_tmap[irow], c = js.kms_cmap[ichan];
+    M2 k0 = give_jones((const float2 *)js.kms, js.kms_dims, js.interp_coefs, t, a0, idir_kms, c, js.interp_mode);
+    M2 k1 = give_jones((const float2 *)js.kms, js.kms_dims, js.interp_coefs, t, a1, idir_kms, c, js.interp_mode);
+    norm_jones(k0, js, u, v);
+    norm_jones(k1, js, u, v);
+    // J = J_kMS . J_beam; without a beam J_beam is the identity (JonesServer.cc:276-289)
+    a = js.beam ? m2_times(k0, a) : k0;
+    b = js.beam ? m2_times(k1, b) : k1;
+  }
+  j0 = a;
+  j1 = b;
+  const float t = (cabs2(a.v[0]) * cabs2(b.v[0]) + cabs2(a.v[3]) * cabs2(b.v[3])) * 0.5f;
+  bb = t * t;
+}
 
 // ----------------------------------------------------------------------------------------
 // Smearing factor (DecorrelationHelper.cc:42-63)
@@ -330,6 +357,56 @@ struct BlockGeom {
   int S;           // support
   unsigned inv;    // ceil(65536 / S): t / S == (t * inv) >> 16 for every tap t < S*S (S <= 63)
   const float2 *cf;  // first tap of the [io][jo] sub-kernel (S*S taps, row-major sy, sx)
+  int cfoff;       // the same tap as an element offset from cf_data
+};
+
+// Footprint of a block packed for a warp broadcast: cell index of the footprint's first tap in
+// the facet grid array, CF element offset, and support with its reciprocal.
+struct TapJob {
+  int base;        // ((band * npol) * ny + locy - sup) * nx + locx - sup
+  int cfoff;
+  int s_inv;       // S | inv << 8
+};
+__device__ __forceinline__ TapJob tap_job(const BlockGeom &g, int band, const ddfg_facet &f) {
+  TapJob j;
+  j.base = ((band * f.npol) * f.ny + g.locy - g.sup) * f.nx + g.locx - g.sup;
+  j.cfoff = g.cfoff;
+  j.s_inv = g.S | (int)(g.inv << 8);
+  return j;
+}
+__device__ __forceinline__ TapJob shfl_job(const TapJob &j, int src) {
+  TapJob o;
+  o.base = __shfl_sync(0xffffffffu, j.base, src);
+  o.cfoff = __shfl_sync(0xffffffffu, j.cfoff, src);
+  o.s_inv = __shfl_sync(0xffffffffu, j.s_inv, src);
+  return o;
+}
+
+// Register slots per lane that hold a footprint of the given support (S*S taps over 32 lanes).
+inline int tap_slots(int max_support) {
+  const int t = max_support * max_support;
+  return t <= 64 ? 2 : (t <= 128 ? 4 : 8);
+}
+
+// Per-lane tap offsets for the current support, recomputed only when the support changes:
+// lane l owns taps t = l + 32 k (k < SLOTS), at cell offset (t / S) * nx + t % S.
+template <int SLOTS>
+struct LaneTaps {
+  int S;
+  int off[SLOTS];
+  __device__ __forceinline__ void reset() { S = -1; }
+  __device__ __forceinline__ void set(int s_inv, int nx, int lane) {
+    const int s = s_inv & 255;
+    if (s == S) return;
+    S = s;
+    const unsigned inv = (unsigned)s_inv >> 8;
+#pragma unroll
+    for (int k = 0; k < SLOTS; ++k) {
+      const int t = lane + 32 * k;
+      const int sy = (int)(((unsigned)t * inv) >> 16);
+      off[k] = (t < s * s) ? sy * nx + (t - sy * s) : -1;
+    }
+  }
 };
 
 __device__ __forceinline__ bool block_geometry(const ddfg_facet &f, double umean, double vmean, double wmean,
@@ -366,7 +443,8 @@ __device__ __forceinline__ bool block_geometry(const ddfg_facet &f, double umean
   g.sup = sup;
   g.S = S;
   g.inv = (65536u + (unsigned)S - 1u) / (unsigned)S;
-  g.cf = (const float2 *)f.cf_data + f.cf_offset[plane] + (int64_t)k * S * S;
+  g.cfoff = (int)(f.cf_offset[plane] + (int64_t)k * S * S);
+  g.cf = (const float2 *)f.cf_data + g.cfoff;
   return true;
 }
 

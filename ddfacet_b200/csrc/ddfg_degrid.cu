@@ -24,73 +24,142 @@
 
 namespace ddfg {
 
-template <int NPOL>
-__global__ void __launch_bounds__(256) degrid_kernel(const ddfg_vis vs, const ddfg_jones js, const FacetPackD pack,
-                                                     const DegridParams dp) {
+// Lane partial sums of the warp's 32 blocks, staged in shared memory and reduced by column:
+// lane j adds the 32 partials of block j (one pass instead of a butterfly per block).
+constexpr int kPartialBytesPerWarp = 32 * 32 * 8;
+
+template <int NPOL, int SLOTS, bool SINGLE>
+__global__ void __launch_bounds__(256) degrid_kernel(const ddfg_vis vs, const ddfg_jones js,
+                                                        const FacetPackD pack, const DegridParams dp) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   ddfg_facet *sf = (ddfg_facet *)smem_raw;
+  float2 *partial = (float2 *)(smem_raw + sizeof(ddfg_facet) * DDFG_FACETS_PER_LAUNCH);
   stage_facets(pack, sf);
   __syncthreads();
   const int lane = threadIdx.x & 31;
   const int warp = threadIdx.x >> 5;
   const int nwarps = blockDim.x >> 5;
   const int64_t nstripes = (vs.nblocks + 31) / 32;
+  float2 *wpart = partial + warp * 32 * 32;   // [block][lane], NPOL == 1 only
+  LaneTaps<SLOTS> lt;
+  lt.reset();
 
   for (int64_t s = (int64_t)blockIdx.x * nwarps + warp; s < nstripes; s += (int64_t)gridDim.x * nwarps) {
     const int64_t b = s * 32 + lane;
     const bool inrange = b < vs.nblocks;
     DegridBlock d;
-    if (inrange) degrid_block_header(vs, b, d);
+    if (inrange && !SINGLE) degrid_block_header(vs, b, d);
     for (int fi = 0; fi < pack.n; ++fi) {
       const ddfg_facet &f = sf[fi];
       BlockGeom g;
-      const bool valid = inrange && degrid_block_geom(vs, f, d, g);
-      const int gridchan = inrange ? d.gridchan : 0;
+      int sch = 0, sgc = 0;
+      int64_t srow = 0;
+      bool valid;
+      if (SINGLE) valid = inrange && degrid_single_geom(vs, f, b, sch, srow, sgc, g);
+      else valid = inrange && degrid_block_geom(vs, f, d, g);
+      TapJob job;
+      if (valid) job = tap_job(g, SINGLE ? sgc : d.gridchan, f);
 
       // Cooperative gather of every valid block's taps (degridder.h:202-212).
       float2 mine[NPOL];
 #pragma unroll
       for (int p = 0; p < NPOL; ++p) mine[p] = czero();
-      const size_t plane_sz = (size_t)f.nx * f.ny;
+      const int plane_sz = f.nx * f.ny;
       const float2 *grid = (const float2 *)f.grid;
-      unsigned mask = __ballot_sync(0xffffffffu, valid);
+      const float2 *cfd = (const float2 *)f.cf_data;
+      const unsigned vmask = __ballot_sync(0xffffffffu, valid);
+      unsigned mask = vmask;
       while (mask) {
-        const int src = __ffs(mask) - 1;
-        mask &= mask - 1;
-        const int locx = __shfl_sync(0xffffffffu, g.locx, src);
-        const int locy = __shfl_sync(0xffffffffu, g.locy, src);
-        const int S = __shfl_sync(0xffffffffu, g.S, src);
-        const unsigned inv = __shfl_sync(0xffffffffu, g.inv, src);
-        const int gch = __shfl_sync(0xffffffffu, gridchan, src);
-        const float2 *cf = (const float2 *)__shfl_sync(0xffffffffu, (unsigned long long)g.cf, src);
-        const int sup = (S - 1) >> 1;
-        const int ntap = S * S;
-        const float2 *g0 = grid + (size_t)gch * f.npol * plane_sz + (size_t)(locy - sup) * f.nx + (locx - sup);
-        float2 acc[NPOL];
+        // Up to four records of equal support at once: their CF and grid loads overlap.
+        int src[4];
+        int nr = 0;
 #pragma unroll
-        for (int p = 0; p < NPOL; ++p) acc[p] = czero();
-        for (int t = lane; t < ntap; t += 32) {
-          const int sy = (int)(((unsigned)t * inv) >> 16);
-          const int sx = t - sy * S;
-          const float2 c = __ldg(cf + t);
-          const float2 *cell = g0 + (size_t)sy * f.nx + sx;
-#pragma unroll
-          for (int p = 0; p < NPOL; ++p) acc[p] = cadd(acc[p], cmul(__ldg(cell + (size_t)p * plane_sz), c));
-        }
-#pragma unroll
-        for (int p = 0; p < NPOL; ++p) {
-#pragma unroll
-          for (int o = 16; o > 0; o >>= 1) {
-            acc[p].x += __shfl_xor_sync(0xffffffffu, acc[p].x, o);
-            acc[p].y += __shfl_xor_sync(0xffffffffu, acc[p].y, o);
+        for (int r = 0; r < 4; ++r) {
+          src[r] = mask ? __ffs(mask) - 1 : -1;
+          if (mask) {
+            mask &= mask - 1;
+            ++nr;
           }
         }
-        if (lane == src) {
+        TapJob j[4];
 #pragma unroll
-          for (int p = 0; p < NPOL; ++p) mine[p] = acc[p];
+        for (int r = 0; r < 4; ++r) j[r] = shfl_job(job, src[r] >= 0 ? src[r] : src[0]);
+        const int S = j[0].s_inv & 255;
+        bool same = S * S <= 32 * SLOTS;
+#pragma unroll
+        for (int r = 1; r < 4; ++r) same = same && (r >= nr || (j[r].s_inv & 255) == S);
+        float2 acc[4][NPOL];
+#pragma unroll
+        for (int r = 0; r < 4; ++r)
+#pragma unroll
+          for (int p = 0; p < NPOL; ++p) acc[r][p] = czero();
+        if (same) {
+          lt.set(j[0].s_inv, f.nx, lane);
+          float2 c[4][SLOTS], gv[4][SLOTS][NPOL];
+#pragma unroll
+          for (int r = 0; r < 4; ++r)
+#pragma unroll
+            for (int k = 0; k < SLOTS; ++k) {
+              const bool on = r < nr && lt.off[k] >= 0;
+              c[r][k] = on ? __ldg(cfd + j[r].cfoff + lane + 32 * k) : czero();
+#pragma unroll
+              for (int p = 0; p < NPOL; ++p)
+                gv[r][k][p] = on ? __ldg(grid + (j[r].base + lt.off[k]) + (size_t)p * plane_sz) : czero();
+            }
+#pragma unroll
+          for (int r = 0; r < 4; ++r)
+#pragma unroll
+            for (int k = 0; k < SLOTS; ++k)
+#pragma unroll
+              for (int p = 0; p < NPOL; ++p) acc[r][p] = cadd(acc[r][p], cmul(gv[r][k][p], c[r][k]));
+        } else {
+          for (int r = 0; r < nr; ++r) {
+            const int Sr = j[r].s_inv & 255;
+            const unsigned inv = (unsigned)j[r].s_inv >> 8;
+            for (int t = lane; t < Sr * Sr; t += 32) {
+              const int sy = (int)(((unsigned)t * inv) >> 16);
+              const float2 cv = __ldg(cfd + j[r].cfoff + t);
+              const float2 *cell = grid + (j[r].base + sy * f.nx + (t - sy * Sr));
+#pragma unroll
+              for (int p = 0; p < NPOL; ++p) acc[r][p] = cadd(acc[r][p], cmul(__ldg(cell + (size_t)p * plane_sz), cv));
+            }
+          }
+        }
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+          if (r >= nr) break;
+          if (NPOL == 1) {
+            wpart[src[r] * 32 + lane] = acc[r][0];
+          } else {
+#pragma unroll
+            for (int p = 0; p < NPOL; ++p) {
+#pragma unroll
+              for (int o = 16; o > 0; o >>= 1) {
+                acc[r][p].x += __shfl_xor_sync(0xffffffffu, acc[r][p].x, o);
+                acc[r][p].y += __shfl_xor_sync(0xffffffffu, acc[r][p].y, o);
+              }
+            }
+            if (lane == src[r]) {
+#pragma unroll
+              for (int p = 0; p < NPOL; ++p) mine[p] = acc[r][p];
+            }
+          }
         }
       }
-      if (valid) degrid_block_apply<NPOL>(vs, js, f, dp, d, mine);
+      if (NPOL == 1) {
+        __syncwarp();
+        if (valid) {
+          float2 t = czero();
+#pragma unroll 8
+          for (int i = 0; i < 32; ++i) t = cadd(t, wpart[lane * 32 + ((i + lane) & 31)]);
+          mine[0] = t;
+        }
+        __syncwarp();
+      }
+      if (valid) {
+        if (SINGLE) degrid_single_apply<NPOL>(vs, js, f, dp, sch, srow, mine);
+        else degrid_block_apply<NPOL>(vs, js, f, dp, d, mine);
+      }
     }
   }
 }
@@ -104,17 +173,35 @@ int ddfg_launch_degrid(const ddfg_vis *vs, const ddfg_jones *js, const ddfg_face
   DegridParams dp;
   dp.policy = policy;
   dp.nvispol = nvispol;
+  int max_support = 1;
+  for (int i = 0; i < nfacets; ++i) max_support = max(max_support, facets[i].max_support);
+  const int slots = tap_slots(max_support);
   for (int f0 = 0; f0 < nfacets; f0 += DDFG_FACETS_PER_LAUNCH) {
     FacetPackD pack;
     pack.n = min(DDFG_FACETS_PER_LAUNCH, nfacets - f0);
     for (int i = 0; i < pack.n; ++i) pack.f[i] = facets[f0 + i];
-    const size_t smem = sizeof(ddfg_facet) * pack.n;
-    switch (nvispol) {
-      case 1: degrid_kernel<1><<<num_ctas, 256, smem, stream>>>(*vs, *js, pack, dp); break;
-      case 2: degrid_kernel<2><<<num_ctas, 256, smem, stream>>>(*vs, *js, pack, dp); break;
-      case 3: degrid_kernel<3><<<num_ctas, 256, smem, stream>>>(*vs, *js, pack, dp); break;
-      default: degrid_kernel<4><<<num_ctas, 256, smem, stream>>>(*vs, *js, pack, dp); break;
-    }
+    const size_t smem = sizeof(ddfg_facet) * DDFG_FACETS_PER_LAUNCH + (nvispol == 1 ? 8 * kPartialBytesPerWarp : 0);
+#define LAUNCH_D1(NP, SL, SG)                                                                                  \
+  do {                                                                                                         \
+    cudaFuncSetAttribute(degrid_kernel<NP, SL, SG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);   \
+    degrid_kernel<NP, SL, SG><<<num_ctas, 256, smem, stream>>>(*vs, *js, pack, dp);                            \
+  } while (0)
+#define LAUNCH_D(NP, SL)                                 \
+  do {                                                   \
+    if (vs->single_vis_blocks) LAUNCH_D1(NP, SL, true);  \
+    else LAUNCH_D1(NP, SL, false);                       \
+  } while (0)
+#define LAUNCH_D_NP(SL)             \
+  switch (nvispol) {                \
+    case 1: LAUNCH_D(1, SL); break; \
+    case 2: LAUNCH_D(2, SL); break; \
+    case 3: LAUNCH_D(3, SL); break; \
+    default: LAUNCH_D(4, SL); break; \
+  }
+    if (slots == 2) { LAUNCH_D_NP(2) } else if (slots == 4) { LAUNCH_D_NP(4) } else { LAUNCH_D_NP(8) }
+#undef LAUNCH_D_NP
+#undef LAUNCH_D
+#undef LAUNCH_D1
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return ddfg_set_error(DDFG_ECUDA, "degrid launch: %s", cudaGetErrorString(e));
   }

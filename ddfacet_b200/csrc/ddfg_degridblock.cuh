@@ -110,4 +110,54 @@ __device__ __forceinline__ void degrid_block_apply(const ddfg_vis &vs, const ddf
   }
 }
 
+// Single-visibility blocks (one row, one channel): degridder.h:138-264 without the loops.
+__device__ __forceinline__ bool degrid_single_geom(const ddfg_vis &vs, const ddfg_facet &f, int64_t b, int &ch,
+                                                   int64_t &irow, int &gridchan, BlockGeom &g) {
+  const int64_t start = vs.block_start[b];
+  ch = vs.bda_map[start];
+  irow = vs.bda_map[start + 2];
+  gridchan = vs.chan_map[ch];
+  if (gridchan < 0 || gridchan >= f.nband) return false;
+  const double *up = vs.uvw + 3 * irow;
+  const double W = up[2];
+  const double um = dadd(up[0], dmul(W, f.cu));
+  const double vm = dadd(up[1], dmul(W, f.cv));
+  const double rw = vs.recip_wvl ? vs.recip_wvl[ch] : vs.freqs[ch] / kC;
+  return block_geometry(f, um, vm, W, rw, g);
+}
+
+template <int NPOL>
+__device__ __forceinline__ void degrid_single_apply(const ddfg_vis &vs, const ddfg_jones &js, const ddfg_facet &f,
+                                                    const DegridParams &dp, int ch, int64_t irow, const float2 *pred) {
+  float2 s[4];
+#pragma unroll
+  for (int p = 0; p < 4; ++p) s[p] = (p < NPOL) ? pred[p] : czero();
+  M2 cv = corr_from_stokes(dp.policy, s);
+  const double *up = vs.uvw + 3 * irow;
+  const double nu = vs.freqs[ch];
+  if (js.mode != 0) {
+    M2 j0, j1;
+    float bb;
+    jones_pair(js, f.idir_kms, f.idir_beam, irow, ch, up[0], up[1], j0, j1, bb);
+    cv = m2_times(m2_times(j0, cv), m2_herm(j1));
+  }
+  const float dec = (float)decorr_factor(vs, f, nu, irow);
+  const double n0m1 = sqrt(1. - f.l0 * f.l0 - f.m0 * f.m0) - 1.;
+  const float2 ph = cscale(phasor_turns(nu * (up[0] * f.l0 + up[1] * f.m0 + up[2] * n0m1) * kInvC), dec);
+  const M2 vb = m2_scale(cv, ph);
+  float2 *vp = (float2 *)vs.vis + (irow * vs.nchan + ch) * (int64_t)vs.ncorr;
+  if (vs.ncorr == 4) {
+    float4 a = *(float4 *)vp, c = *(float4 *)(vp + 2);
+    a.x -= vb.v[0].x; a.y -= vb.v[0].y; a.z -= vb.v[1].x; a.w -= vb.v[1].y;
+    c.x -= vb.v[2].x; c.y -= vb.v[2].y; c.z -= vb.v[3].x; c.w -= vb.v[3].y;
+    *(float4 *)vp = a;
+    *(float4 *)(vp + 2) = c;
+  } else if (vs.ncorr == 2) {
+    vp[0] = csub(vp[0], vb.v[0]);
+    vp[1] = csub(vp[1], vb.v[3]);
+  } else {
+    vp[0] = csub(vp[0], vb.v[0]);
+  }
+}
+
 }  // namespace ddfg

@@ -24,7 +24,7 @@
 
 namespace ddfg {
 
-template <int NPOL>
+template <int NPOL, int SLOTS, bool SINGLE>
 __global__ void __launch_bounds__(256) grid_kernel(const ddfg_vis vs, const ddfg_jones js, const FacetPack pack,
                                                    const GridParams gp) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -50,45 +50,90 @@ __global__ void __launch_bounds__(256) grid_kernel(const ddfg_vis vs, const ddfg
 
     const double n0m1 = sqrt(1. - f.l0 * f.l0 - f.m0 * f.m0) - 1.;
     float2 *grid = (float2 *)f.grid;
-    const size_t plane_sz = (size_t)f.nx * f.ny;
+    const float2 *cfd = (const float2 *)f.cf_data;
+    const int plane_sz = f.nx * f.ny;
     JonesCache jc;
+    LaneTaps<SLOTS> lt;
+    lt.reset();
 
     for (int64_t s = (int64_t)blockIdx.x * nwarps + warp; s < nstripes; s += (int64_t)gridDim.x * nwarps) {
       const int64_t b = s * 32 + lane;
       GridRecord<NPOL> rec;
       rec.valid = false;
-      if (b < vs.nblocks) grid_block_record<NPOL>(vs, js, f, gp, b, n0m1, rec, jc);
+      if (b < vs.nblocks) {
+        if (SINGLE) grid_single_record<NPOL>(vs, js, f, gp, b, n0m1, rec);
+        else grid_block_record<NPOL>(vs, js, f, gp, b, n0m1, rec, jc);
+      }
 
-      warp_add_block_sums<NPOL>(vs, js, f, gp, b, rec, npol_used, s_sumwt, s_sumj, s_chan, jc);
+      warp_add_block_sums<NPOL, SINGLE>(vs, js, f, gp, b, rec, npol_used, s_sumwt, s_sumj, s_chan, jc);
 
-      // Warp-cooperative tap scatter of the 32 records (gridder.h:353-362).
+      // Warp-cooperative tap scatter of the 32 records (gridder.h:353-362): the record's
+      // footprint, CF offset and support travel in three shuffles; each lane keeps the cell
+      // offsets of its taps for as long as the support stays the same.  Up to four records of
+      // equal support are issued together so their CF loads are in flight at once.
+      TapJob job;
+      if (rec.valid) job = tap_job(rec.g, rec.gridchan, f);
       unsigned mask = __ballot_sync(0xffffffffu, rec.valid);
       while (mask) {
-        const int src = __ffs(mask) - 1;
-        mask &= mask - 1;
-        const int locx = __shfl_sync(0xffffffffu, rec.g.locx, src);
-        const int locy = __shfl_sync(0xffffffffu, rec.g.locy, src);
-        const int S = __shfl_sync(0xffffffffu, rec.g.S, src);
-        const unsigned inv = __shfl_sync(0xffffffffu, rec.g.inv, src);
-        const int gch = __shfl_sync(0xffffffffu, rec.gridchan, src);
-        const float2 *cf = (const float2 *)__shfl_sync(0xffffffffu, (unsigned long long)rec.g.cf, src);
-        float2 sv[NPOL];
+        int src[4];
+        int nr = 0;
 #pragma unroll
-        for (int p = 0; p < NPOL; ++p) {
-          sv[p].x = __shfl_sync(0xffffffffu, rec.stokes[p].x, src);
-          sv[p].y = __shfl_sync(0xffffffffu, rec.stokes[p].y, src);
+        for (int r = 0; r < 4; ++r) {
+          src[r] = mask ? __ffs(mask) - 1 : -1;
+          if (mask) {
+            mask &= mask - 1;
+            ++nr;
+          }
         }
-        const int sup = (S - 1) >> 1;
-        const int ntap = S * S;
-        float2 *g0 = grid + (size_t)gch * f.npol * plane_sz + (size_t)(locy - sup) * f.nx + (locx - sup);
-        for (int t = lane; t < ntap; t += 32) {
-          const int sy = (int)(((unsigned)t * inv) >> 16);
-          const int sx = t - sy * S;
-          const float2 c = __ldg(cf + t);
-          float2 *cell = g0 + (size_t)sy * f.nx + sx;
+        TapJob j[4];
+        float2 sv[4][NPOL];
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+          const int sr = src[r] >= 0 ? src[r] : src[0];
+          j[r] = shfl_job(job, sr);
 #pragma unroll
           for (int p = 0; p < NPOL; ++p) {
-            if (p < npol_used) atomicAdd(cell + (size_t)p * plane_sz, cmul(sv[p], c));
+            sv[r][p].x = __shfl_sync(0xffffffffu, rec.stokes[p].x, sr);
+            sv[r][p].y = __shfl_sync(0xffffffffu, rec.stokes[p].y, sr);
+          }
+        }
+        const int S = j[0].s_inv & 255;
+        bool same = S * S <= 32 * SLOTS;
+#pragma unroll
+        for (int r = 1; r < 4; ++r) same = same && (r >= nr || (j[r].s_inv & 255) == S);
+        if (same) {
+          lt.set(j[0].s_inv, f.nx, lane);
+          float2 c[4][SLOTS];
+#pragma unroll
+          for (int r = 0; r < 4; ++r)
+#pragma unroll
+            for (int k = 0; k < SLOTS; ++k)
+              c[r][k] = (r < nr && lt.off[k] >= 0) ? __ldg(cfd + j[r].cfoff + lane + 32 * k) : czero();
+#pragma unroll
+          for (int r = 0; r < 4; ++r) {
+            if (r >= nr) break;
+#pragma unroll
+            for (int k = 0; k < SLOTS; ++k) {
+              if (lt.off[k] >= 0) {
+                float2 *cell = grid + (j[r].base + lt.off[k]);
+#pragma unroll
+                for (int p = 0; p < NPOL; ++p)
+                  if (p < npol_used) atomicAdd(cell + (size_t)p * plane_sz, cmul(sv[r][p], c[r][k]));
+              }
+            }
+          }
+        } else {
+          for (int r = 0; r < nr; ++r) {
+            const int Sr = j[r].s_inv & 255;
+            const unsigned inv = (unsigned)j[r].s_inv >> 8;
+            for (int t = lane; t < Sr * Sr; t += 32) {
+              const int sy = (int)(((unsigned)t * inv) >> 16);
+              const float2 cv = __ldg(cfd + j[r].cfoff + t);
+              float2 *cell = grid + (j[r].base + sy * f.nx + (t - sy * Sr));
+#pragma unroll
+              for (int p = 0; p < NPOL; ++p)
+                if (p < npol_used) atomicAdd(cell + (size_t)p * plane_sz, cmul(sv[r][p], cv));
+            }
           }
         }
       }
@@ -113,6 +158,9 @@ using namespace ddfg;
 
 int ddfg_launch_grid(const ddfg_vis *vs, const ddfg_jones *js, const ddfg_facet *facets, int nfacets, int policy,
                      int nvispol, int dopsf, int num_ctas, cudaStream_t stream) {
+  int max_support = 1;
+  for (int i = 0; i < nfacets; ++i) max_support = max(max_support, facets[i].max_support);
+  const int slots = tap_slots(max_support);
   GridParams gp;
   gp.policy = policy;
   gp.nvispol = nvispol;
@@ -128,19 +176,28 @@ int ddfg_launch_grid(const ddfg_vis *vs, const ddfg_jones *js, const ddfg_facet 
     for (int i = 0; i < pack.n; ++i) pack.f[i] = facets[f0 + i];
     const int npol = nvispol;
     cudaError_t e;
-#define LAUNCH_G(NP)                                                                                   \
-  do {                                                                                                 \
-    if (smem > 48 * 1024)                                                                              \
-      cudaFuncSetAttribute(grid_kernel<NP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);   \
-    grid_kernel<NP><<<num_ctas, 256, smem, stream>>>(*vs, *js, pack, gp);                              \
+#define LAUNCH_G1(NP, SL, SG)                                                                                 \
+  do {                                                                                                        \
+    if (smem > 48 * 1024)                                                                                     \
+      cudaFuncSetAttribute(grid_kernel<NP, SL, SG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);  \
+    grid_kernel<NP, SL, SG><<<num_ctas, 256, smem, stream>>>(*vs, *js, pack, gp);                             \
   } while (0)
-    switch (npol) {
-      case 1: LAUNCH_G(1); break;
-      case 2: LAUNCH_G(2); break;
-      case 3: LAUNCH_G(3); break;
-      default: LAUNCH_G(4); break;
-    }
+#define LAUNCH_G(NP, SL)                                 \
+  do {                                                   \
+    if (vs->single_vis_blocks) LAUNCH_G1(NP, SL, true);  \
+    else LAUNCH_G1(NP, SL, false);                       \
+  } while (0)
+#define LAUNCH_G_NP(SL)            \
+  switch (npol) {                  \
+    case 1: LAUNCH_G(1, SL); break; \
+    case 2: LAUNCH_G(2, SL); break; \
+    case 3: LAUNCH_G(3, SL); break; \
+    default: LAUNCH_G(4, SL); break; \
+  }
+    if (slots == 2) { LAUNCH_G_NP(2) } else if (slots == 4) { LAUNCH_G_NP(4) } else { LAUNCH_G_NP(8) }
+#undef LAUNCH_G_NP
 #undef LAUNCH_G
+#undef LAUNCH_G1
     e = cudaGetLastError();
     if (e != cudaSuccess) return ddfg_set_error(DDFG_ECUDA, "grid launch: %s", cudaGetErrorString(e));
   }

@@ -30,6 +30,80 @@ struct GridRecord {
   bool single_chan;       // one channel: its channel sums are the block sums
 };
 
+// A block of exactly one row and one channel (every block of a map built without averaging):
+// the walk of gridder.h:184-351 with its loops, means and cache collapsed.  Sums over one term
+// equal that term exactly (0 + x == x, x / 1 == x), so the FP64 index inputs are the same.
+template <int NPOL>
+__device__ __forceinline__ void grid_single_record(const ddfg_vis &vs, const ddfg_jones &js, const ddfg_facet &f,
+                                                   const GridParams &gp, int64_t b, double n0m1,
+                                                   GridRecord<NPOL> &rec) {
+  rec.valid = false;
+  if (vs.sparsification && !vs.sparsification[b]) return;
+  const int64_t start = vs.block_start[b];
+  const int ch = vs.bda_map[start];
+  const int64_t irow = vs.bda_map[start + 2];
+  const int64_t doff = (irow * vs.nchan + ch) * (int64_t)vs.ncorr;
+  if (vs.flags[doff]) return;
+  const int gridchan = vs.chan_map[ch];
+  if (gridchan < 0 || gridchan >= f.nband) return;
+  const double U = vs.uvw[3 * irow], V = vs.uvw[3 * irow + 1], W = vs.uvw[3 * irow + 2];
+  const double umean = dadd(U, dmul(W, f.cu));
+  const double vmean = dadd(V, dmul(W, f.cv));
+  const double recip = vs.recip_wvl ? vs.recip_wvl[ch] : vs.freqs[ch] / kC;
+  if (!block_geometry(f, umean, vmean, W, recip, rec.g)) return;
+
+  const double nu = vs.freqs[ch];
+  const double dec = decorr_factor(vs, f, gp.freq_mean0, irow);
+  const float decf = (float)dec;
+  M2 vm;
+  if (gp.dopsf) {
+    vm.v[0] = make_float2(decf, 0.f); vm.v[1] = czero(); vm.v[2] = czero(); vm.v[3] = make_float2(decf, 0.f);
+  } else {
+    const float2 *vp = (const float2 *)vs.vis + doff;
+    if (vs.ncorr == 4) {
+      const float4 a = *(const float4 *)vp, c = *(const float4 *)(vp + 2);
+      vm.v[0] = make_float2(a.x, a.y); vm.v[1] = make_float2(a.z, a.w);
+      vm.v[2] = make_float2(c.x, c.y); vm.v[3] = make_float2(c.z, c.w);
+    } else if (vs.ncorr == 2) {
+      vm.v[0] = vp[0]; vm.v[1] = czero(); vm.v[2] = czero(); vm.v[3] = vp[1];
+    } else {
+      vm.v[0] = vp[0]; vm.v[1] = czero(); vm.v[2] = czero(); vm.v[3] = vp[0];
+    }
+  }
+  const double fw = (double)vs.weights[irow * vs.nchan + ch];
+  const double fwd = fw * dec * dec;
+  double sumjones = 0.;
+  if (js.mode != 0) {
+    M2 j0, j1;
+    float bb;
+    // mode 1 normalises with the row's uvw, mode 2 with the block mean (gridder.h:236, 294)
+    jones_pair(js, f.idir_kms, f.idir_beam, irow, ch, js.mode == 1 ? U : umean, js.mode == 1 ? V : vmean, j0, j1, bb);
+    // PSF: J0^H J0 J1^H J1 times the smearing factor in both modes (gridder.h:236-242, 295-297)
+    if (gp.dopsf) vm = m2_scale(m2_times(m2_times(m2_herm(j0), m2_times(j0, m2_herm(j1))), j1), make_float2(decf, 0.f));
+    else vm = m2_times(m2_times(m2_herm(j0), vm), j1);
+    sumjones = (double)bb * fwd;
+  }
+  const float2 corr = gp.dopsf ? make_float2(1.f, 0.f)
+                               : phasor_turns(-nu * (U * f.l0 + V * f.m0 + W * n0m1) * kInvC);
+  const float2 wgt = cscale(corr, (float)fw);
+  M2 acc;
+  acc.v[0] = cmul(vm.v[0], wgt);
+  acc.v[1] = vs.ncorr == 4 ? cmul(vm.v[1], wgt) : czero();
+  acc.v[2] = vs.ncorr == 4 ? cmul(vm.v[2], wgt) : czero();
+  acc.v[3] = vs.ncorr >= 2 ? cmul(vm.v[3], wgt) : czero();
+  float2 st[4];
+  stokes_from_corr(gp.policy, acc, st);
+#pragma unroll
+  for (int p = 0; p < NPOL; ++p) rec.stokes[p] = st[p];
+  rec.valid = true;
+  rec.gridchan = gridchan;
+  rec.weight = fw;
+  rec.sumjones = sumjones;
+  rec.sumsqw = fwd;
+  rec.ch0 = ch;
+  rec.single_chan = true;
+}
+
 // Walk one block for one facet: gridder.h:184-351.
 template <int NPOL>
 __device__ __forceinline__ void grid_block_record(const ddfg_vis &vs, const ddfg_jones &js, const ddfg_facet &f,
@@ -209,7 +283,7 @@ __device__ __forceinline__ void grid_block_add_chan_sums(const ddfg_vis &vs, con
 // The warp's 32 records' contributions to the weight and Jones sums (gridder.h:363-373): one
 // shared-memory update per warp when every valid lane grids into the same band, per lane
 // otherwise.  Must be called by all 32 lanes.
-template <int NPOL>
+template <int NPOL, bool SINGLE = false>
 __device__ __forceinline__ void warp_add_block_sums(const ddfg_vis &vs, const ddfg_jones &js, const ddfg_facet &f,
                                                     const GridParams &gp, int64_t b, const GridRecord<NPOL> &rec,
                                                     int npol_used, double *a_sumwt, double *a_sumj, double *a_chan,
@@ -238,7 +312,14 @@ __device__ __forceinline__ void warp_add_block_sums(const ddfg_vis &vs, const dd
       atomicAdd(&a_sumj[f.nband + g], (double)npol_used * qsum);
     }
   }
-  if (js.mode != 0 && rec.valid) grid_block_add_chan_sums<NPOL>(vs, js, f, gp, b, rec, (double)npol_used, a_chan, jc);
+  if (js.mode != 0 && rec.valid) {
+    if (SINGLE) {
+      atomicAdd(&a_chan[rec.ch0], (double)npol_used * rec.sumjones);
+      atomicAdd(&a_chan[vs.nchan + rec.ch0], (double)npol_used * rec.sumsqw);
+    } else {
+      grid_block_add_chan_sums<NPOL>(vs, js, f, gp, b, rec, (double)npol_used, a_chan, jc);
+    }
+  }
 }
 
 }  // namespace ddfg

@@ -71,6 +71,7 @@ class VisData:
     block_start: torch.Tensor    # int64 [nblocks]
     nblocks: int
     chan_equidistant: int
+    single_vis_blocks: int = 0
     sparsification: Optional[torch.Tensor] = None
     uvw_dt: Optional[torch.Tensor] = None
     dt: float = 0.0
@@ -79,16 +80,19 @@ class VisData:
     do_fsmear: int = 0
 
     @staticmethod
-    def plan_map(bda_map: torch.Tensor, nrow: int, nchan: int, stream=None) -> torch.Tensor:
-        """Block starts of a packed BDA map (checked); see ddfg_bda_plan."""
+    def plan_map(bda_map: torch.Tensor, nrow: int, nchan: int, stream=None):
+        """(block starts, every-block-single-visibility flag) of a packed BDA map (checked);
+        see ddfg_bda_plan."""
         lib = _abi.lib()
         m = bda_map
-        nb = int(m[0].item()) + (int(m[1].item()) << 32) if m.is_cuda else int(m[0]) + (int(m[1]) << 32)
+        lo, hi = (int(x) for x in m[:2].cpu().numpy().view(np.uint32)) if m.is_cuda else (int(np.uint32(m[0])), int(m[1]))
+        nb = lo + (hi << 32)
         starts = torch.empty(max(nb, 1), dtype=torch.int64, device=m.device)
         ws = torch.empty(int(lib.ddfg_bda_plan_workspace_size(nb)), dtype=torch.uint8, device=m.device)
+        single = C.c_int32(0)
         _abi.check(lib.ddfg_bda_plan(m.data_ptr(), m.numel(), nb, nrow, nchan, starts.data_ptr(), ws.data_ptr(),
-                                     ws.numel(), _stream_ptr(stream)))
-        return starts[:nb] if nb > 0 else starts[:0]
+                                     ws.numel(), _stream_ptr(stream), C.byref(single)))
+        return (starts[:nb] if nb > 0 else starts[:0]), int(single.value)
 
     @classmethod
     def create(cls, vis, uvw, flags, weights, freqs, chan_map, bda_map, device=None, sparsification=None,
@@ -111,8 +115,9 @@ class VisData:
             f = f.view(torch.uint8)
         fl = to_device(f, torch.uint8, device, non_blocking=non_blocking)
         bm = to_device(bda_map, torch.int32, device, non_blocking=non_blocking)
+        single = 0
         if block_start is None:
-            block_start = cls.plan_map(bm, nrow, nchan)
+            block_start, single = cls.plan_map(bm, nrow, nchan)
         nb = int(block_start.numel())
         sp = None
         if sparsification is not None and np.size(sparsification) > 0:
@@ -134,6 +139,7 @@ class VisData:
             block_start=block_start,
             nblocks=nb,
             chan_equidistant=cheq,
+            single_vis_blocks=single,
             sparsification=sp,
         )
         if smear is not None and len(smear) > 0:
@@ -155,6 +161,7 @@ class VisData:
         s.chan_map = self.chan_map.data_ptr()
         s.nrow, s.nchan, s.ncorr = nrow, nchan, ncorr
         s.chan_equidistant = self.chan_equidistant
+        s.single_vis_blocks = int(self.single_vis_blocks)
         s.bda_map = self.bda_map.data_ptr()
         s.bda_len = self.bda_map.numel()
         s.block_start = self.block_start.data_ptr() if self.nblocks > 0 else None

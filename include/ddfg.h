@@ -79,6 +79,8 @@ typedef struct ddfg_vis {
   int64_t nrow;
   int32_t nchan, ncorr;
   int32_t chan_equidistant;    /* LOptimisation[1]                                        */
+  int32_t single_vis_blocks;   /* 1 only if every block is one row x one channel, as
+                                  ddfg_bda_plan reports it; selects the lighter kernels    */
   const int32_t *bda_map;      /* packed block map                                        */
   int64_t bda_len;             /* words in bda_map                                        */
   const int64_t *block_start;  /* [nblocks] word index of each block's [ch0,ch1,rows...]  */
@@ -134,14 +136,17 @@ int ddfg_last_error(char *buf, int len);
 /* Bytes of device scratch ddfg_bda_plan needs for a map of nblocks blocks. */
 size_t ddfg_bda_plan_workspace_size(int64_t nblocks);
 
-/* Reads the map's block sizes, writes the word index of every block record into block_start
+/* single_out (host, may be NULL) receives 1 when every block has exactly one row and one
+ * channel (the map of unaveraged data), else 0.
+ * Reads the map's block sizes, writes the word index of every block record into block_start
  * (device, int64 [nblocks]) and checks that the header's block count is nblocks, every block
  * lies inside the map, 0 <= ch0 <= ch1 <= nchan and every row is in [0, nrow).  A plan call,
  * not a hot one: it synchronises the stream to read the check's result, and returns DDFG_EMAP
  * for a malformed map.  Replaces the sequential block walk of gridder.h:144-148, 185-190 and
  * degridder.h:107-136. */
 int ddfg_bda_plan(const int32_t *bda_map, int64_t bda_len, int64_t nblocks, int64_t nrow, int32_t nchan,
-                  int64_t *block_start, void *workspace, size_t workspace_bytes, void *stream);
+                  int64_t *block_start, void *workspace, size_t workspace_bytes, void *stream,
+                  int32_t *single_out);
 
 /* Grid the visibility set onto every facet's grid (accumulating), with W-projection, facet
  * phase shift, per-antenna Jones, smearing and corr->Stokes conversion.
@@ -158,6 +163,20 @@ int ddfg_grid(const ddfg_vis *vs, const ddfg_jones *js, const ddfg_pol *pol,
  * facet of a call is applied by the warp that owns the block, so the result is deterministic. */
 int ddfg_degrid(const ddfg_vis *vs, const ddfg_jones *js, const ddfg_pol *pol,
                 const ddfg_facet *facets, int nfacets, void *stream);
+
+/* Most blocks ddfg_bda_plan_noalloc accepts. */
+#define DDFG_BDA_PLAN_NOALLOC_MAX_BLOCKS (1 << 24)
+
+/* ddfg_bda_plan for callers that cannot allocate device memory.  It has no counterpart in the
+ * reference.  Same inputs, outputs and checks as ddfg_bda_plan, but no workspace argument: its
+ * scratch is a fixed 1 MiB array inside the library, held by every GPU that loads the library
+ * until the process exits, so maps are limited to DDFG_BDA_PLAN_NOALLOC_MAX_BLOCKS blocks
+ * (DDFG_ESIZE above that).  It allocates nothing.  Its first call on a device looks up that
+ * array's device address (with the device current), so make that first call before any stream
+ * capture.  Calls share the array: calls that overlap on the GPU race and must be serialised by
+ * the caller. */
+int ddfg_bda_plan_noalloc(const int32_t *bda_map, int64_t bda_len, int64_t nblocks, int64_t nrow, int32_t nchan,
+                          int64_t *block_start, void *stream, int32_t *single_out);
 
 /* Device scratch of ddfg_sort_plan_build (bytes). */
 size_t ddfg_sort_plan_workspace_size(int64_t nblocks);

@@ -1,0 +1,156 @@
+"""ctypes driver of the FP64 gridder/degridder restatement (test infrastructure only).
+
+``grid(case, ...)`` and ``degrid(case, model, ...)`` run oracle/gridder_fp64.c on the same
+inputs as the GPU path and the reference module, accumulating in complex128.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "_build", "libddfg_fp64.so")
+_lib = None
+
+_vp = C.c_void_p
+
+
+class JonesIn(C.Structure):
+    _fields_ = [("mode", C.c_int), ("kms", _vp), ("kdims", C.c_int * 4), ("ktmap", _vp), ("kcmap", _vp),
+                ("beam", _vp), ("bdims", C.c_int * 4), ("btmap", _vp), ("bcmap", _vp), ("a0", _vp), ("a1", _vp),
+                ("idir_kms", C.c_int), ("idir_beam", C.c_int), ("coefs", _vp), ("interp_mode", C.c_int),
+                ("apply_amp", C.c_int), ("apply_phase", C.c_int), ("scale", C.c_int), ("calib_err", C.c_double),
+                ("wl_mean", C.c_double)]
+
+
+class SmearIn(C.Structure):
+    _fields_ = [("uvw_dt", _vp), ("dt", C.c_double), ("dnu", C.c_double), ("l", C.c_double), ("m", C.c_double),
+                ("do_t", C.c_int), ("do_f", C.c_int)]
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB):
+            subprocess.run(["bash", os.path.join(HERE, "build_fp64.sh")], check=True)
+        _lib = C.CDLL(LIB)
+    return _lib
+
+
+def _p(a):
+    return C.c_void_p(None if a is None else a.ctypes.data)
+
+
+def _pack_cf(wplanes, wconj, overs, degrid):
+    first, second = (wconj, wplanes) if degrid else (wplanes, wconj)
+    planes = list(first) + list(second)
+    sizes = [p.size for p in planes]
+    off = np.concatenate([[0], np.cumsum(sizes)[:-1]]).astype(np.int64)
+    data = np.concatenate([np.ascontiguousarray(p, np.complex64).ravel() for p in planes])
+    sup = np.array([p.shape[0] // overs for p in planes], np.int32)
+    return data, off, sup
+
+
+def _jones(j, keep):
+    ji = JonesIn()
+    if not j:
+        ji.mode = 0
+        return ji
+    ji.mode = int(j["mode"])
+    for key, dims, tm, cm in (("kms", "kdims", "ktmap", "kcmap"), ("beam", "bdims", "btmap", "bcmap")):
+        if key in j:
+            arr = np.ascontiguousarray(j[key], np.complex64)
+            keep.append(arr)
+            setattr(ji, key, arr.ctypes.data)
+            for i in range(4):
+                getattr(ji, dims)[i] = arr.shape[i]
+            t = np.ascontiguousarray(j[key + "_tmap"], np.int32)
+            c = np.ascontiguousarray(j[key + "_cmap"], np.int32)
+            keep += [t, c]
+            setattr(ji, tm, t.ctypes.data)
+            setattr(ji, cm, c.ctypes.data)
+    a0 = np.ascontiguousarray(j["A0"], np.int32)
+    a1 = np.ascontiguousarray(j["A1"], np.int32)
+    keep += [a0, a1]
+    ji.a0, ji.a1 = a0.ctypes.data, a1.ctypes.data
+    ji.idir_kms, ji.idir_beam = int(j.get("idir_kms", 0)), int(j.get("idir_beam", 0))
+    if "coefs" in j:
+        co = np.ascontiguousarray(j["coefs"], np.float32)
+        keep.append(co)
+        ji.coefs = co.ctypes.data
+    ji.interp_mode = int(j.get("interp_mode", 0))
+    ji.apply_amp, ji.apply_phase, ji.scale = int(j.get("apply_amp", 1)), int(j.get("apply_phase", 1)), int(j.get("scale", 0))
+    ji.calib_err = float(j.get("calib_err", 0.0))
+    ji.wl_mean = float(j.get("wl_mean", 1.0))
+    return ji
+
+
+def _smear(s, keep):
+    si = SmearIn()
+    if s:
+        dt = np.ascontiguousarray(s[0], np.float64)
+        keep.append(dt)
+        si.uvw_dt = dt.ctypes.data
+        si.dt, si.dnu, si.do_t, si.do_f, si.l, si.m = float(s[1]), float(s[2]), int(s[3]), int(s[4]), float(s[5]), float(s[6])
+    return si
+
+
+def grid(vis, uvw, flags, weights, freqs, chan_map, bda_map, wplanes, wconj, overs, ref_wave, wmax, incr, cu, cv, lm,
+         corr_ids, stokes_ids, nband, npix, jones=None, smear=None, dopsf=False, sparsification=None):
+    """FP64 grid [nband, npol, npix, npix] complex128, sumwt, sumjones, sumjones_chan."""
+    keep = []
+    npol = len(stokes_ids)
+    nrow, nchan, ncorr = vis.shape
+    g = np.zeros((nband, npol, npix, npix), np.complex128)
+    sumwt = np.zeros((nband, npol))
+    sj = np.zeros((2, nband))
+    sjc = np.zeros((2, nchan))
+    cf, off, sup = _pack_cf(wplanes, wconj, overs, degrid=False)
+    arrs = [np.ascontiguousarray(vis, np.complex64), np.ascontiguousarray(uvw, np.float64),
+            np.ascontiguousarray(flags).view(np.uint8) if flags.dtype == bool else np.ascontiguousarray(flags, np.uint8),
+            np.ascontiguousarray(weights, np.float32), np.ascontiguousarray(freqs, np.float64),
+            np.ascontiguousarray(chan_map, np.int32), np.ascontiguousarray(bda_map, np.int32),
+            np.array(corr_ids, np.int32), np.array(stokes_ids, np.int32)]
+    sp = None if sparsification is None else np.ascontiguousarray(sparsification, np.uint8)
+    if jones:
+        jones = dict(jones, wl_mean=float(np.mean(299792458.0 / np.asarray(freqs))))
+    ji, si = _jones(jones, keep), _smear(smear, keep)
+    f = lib().fp64_grid
+    f.restype = C.c_int
+    rc = f(_p(g), nband, npol, npix, npix, _p(arrs[0]), _p(arrs[1]), _p(arrs[2]), _p(arrs[3]), C.c_int64(nrow), nchan,
+           ncorr, _p(arrs[4]), _p(arrs[5]), _p(arrs[6]), _p(cf), _p(off), _p(sup), len(wplanes), int(overs),
+           C.c_double(ref_wave), C.c_double(wmax), C.c_double(incr[0]), C.c_double(incr[1]), C.c_double(cu),
+           C.c_double(cv), C.c_double(lm[0]), C.c_double(lm[1]), _p(arrs[7]), len(corr_ids), _p(arrs[8]),
+           len(stokes_ids), int(bool(dopsf)), C.byref(ji), C.byref(si), _p(sp), _p(sumwt), _p(sj), _p(sjc))
+    if rc:
+        raise ValueError("unsupported correlation/Stokes combination")
+    return g, sumwt, sj, sjc
+
+
+def degrid(model, vis0, uvw, freqs, chan_map, bda_map, wplanes, wconj, overs, ref_wave, wmax, incr, cu, cv, lm, corr_ids,
+           stokes_ids, jones=None, smear=None):
+    """vis0 - prediction, complex128 [nrow, nchan, ncorr]."""
+    keep = []
+    nband, npol, ny, nx = model.shape
+    nrow, nchan, ncorr = vis0.shape
+    v = np.ascontiguousarray(vis0, np.complex128).copy()
+    cf, off, sup = _pack_cf(wplanes, wconj, overs, degrid=True)
+    m = np.ascontiguousarray(model, np.complex64)
+    arrs = [np.ascontiguousarray(uvw, np.float64), np.ascontiguousarray(freqs, np.float64),
+            np.ascontiguousarray(chan_map, np.int32), np.ascontiguousarray(bda_map, np.int32),
+            np.array(corr_ids, np.int32), np.array(stokes_ids, np.int32)]
+    if jones:
+        jones = dict(jones, wl_mean=float(np.mean(299792458.0 / np.asarray(freqs))))
+    ji, si = _jones(jones, keep), _smear(smear, keep)
+    f = lib().fp64_degrid
+    f.restype = C.c_int
+    rc = f(_p(m), nband, npol, ny, nx, _p(v), _p(arrs[0]), C.c_int64(nrow), nchan, ncorr, _p(arrs[1]), _p(arrs[2]),
+           _p(arrs[3]), _p(cf), _p(off), _p(sup), len(wplanes), int(overs), C.c_double(ref_wave), C.c_double(wmax),
+           C.c_double(incr[0]), C.c_double(incr[1]), C.c_double(cu), C.c_double(cv), C.c_double(lm[0]),
+           C.c_double(lm[1]), _p(arrs[4]), len(corr_ids), _p(arrs[5]), len(stokes_ids), C.byref(ji), C.byref(si))
+    if rc:
+        raise ValueError("unsupported correlation/Stokes combination")
+    return v

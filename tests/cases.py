@@ -204,3 +204,22 @@ def rel_rms(a, b):
     b = np.asarray(b, np.complex128)
     den = np.sqrt(np.mean(np.abs(b) ** 2))
     return float(np.sqrt(np.mean(np.abs(a - b) ** 2)) / (den if den > 0 else 1.0))
+
+
+def run_fp64_grid(c, dopsf=False, sparsification=None):
+    from oracle import fp64
+
+    g, sw, sj, sjc = fp64.grid(c.vis, c.uvw, c.flags, c.weights, c.freqs, c.chan_map, c.bda, c.wt.Wplanes,
+                               c.wt.WplanesConj, c.winfos[3], c.wt.RefWave, c.wt.wmax, c.incr, c.wt.Cu, c.wt.Cv, c.lm,
+                               c.corr_ids, c.stokes_ids, c.nband, c.npix, jones=c.jones, smear=c.smear, dopsf=dopsf,
+                               sparsification=sparsification)
+    return {"grid": g, "sumwt": sw, "sumjones": sj, "sumjones_chan": sjc}
+
+
+def run_fp64_degrid(c, model_grid, vis0=None):
+    from oracle import fp64
+
+    v0 = np.zeros_like(c.vis) if vis0 is None else vis0
+    return fp64.degrid(model_grid, v0, c.uvw, c.freqs, c.chan_map, c.bda, c.wt.Wplanes, c.wt.WplanesConj, c.winfos[3],
+                       c.wt.RefWave, c.wt.wmax, c.incr, c.wt.Cu, c.wt.Cv, c.lm, c.corr_ids, c.stokes_ids,
+                       jones=c.jones, smear=c.smear)
