@@ -202,6 +202,41 @@ int ddfg_grid_sorted(const ddfg_vis *vs, const ddfg_jones *js, const ddfg_pol *p
 int ddfg_degrid_sorted(const ddfg_vis *vs, const ddfg_jones *js, const ddfg_pol *pol, const ddfg_facet *facets,
                        int nfacets, const ddfg_sort_plan *plan, int facets_per_launch, void *stream);
 
+/* ---- per-facet transforms and stitching --------------------------------------------- */
+
+/* A batched N x N complex64 FFT plan (cuFFT).  Creating one allocates; using one does not. */
+typedef struct ddfg_fft_plan ddfg_fft_plan;
+int ddfg_fft_plan_create(int32_t n, int32_t batch, ddfg_fft_plan **out);
+int ddfg_fft_plan_destroy(ddfg_fft_plan *plan);
+
+/* GridToIm in place on grid[batch][N][N] (ClassDDEGridMachine.py:1186-1190, ModFFTW.py:584-599):
+ * grid <- fftshift(IDFT(ifftshift(grid * scale))) with the unnormalised inverse DFT (numpy's
+ * ifft2 times N^2); scale is OverS^2 for GridToIm.  work: a second [batch][N][N] buffer. */
+int ddfg_grid_to_image(ddfg_fft_plan *plan, void *grid, double scale, void *work, void *stream);
+
+/* Adds one facet's dirty image (complex64 [nband][npol][N][N] from ddfg_grid_to_image) into the
+ * main image float32 [nband][npol][M][M] (FacetsToIm_Channel, ClassFacetMachine.py:1331-1410):
+ * Re(dirty) * invsphe * sw_grid / weights[band][pol] (weights 0 counts as 1), zero where
+ * sphe < 1e-3, flipped and transposed, cropped by GiveEdges around the facet centre pixel
+ * (xc, yc).  sphe, invsphe (float32 of 1/taper) and sw_grid are [N][N] in grid orientation;
+ * weights is float64
+ * [nband][npol] = SumWeights * sqrt(SumJonesNorm). */
+int ddfg_stitch_facet(const void *dirty, int32_t nband, int32_t npol, int32_t n, const float *sphe,
+                      const float *invsphe, const float *sw_grid, const double *weights, float *image, int32_t m,
+                      int32_t xc, int32_t yc, void *stream);
+
+/* image[plane] /= facet_norm (ClassFacetMachine.py:1411-1414); facet_norm is [M][M]. */
+int ddfg_image_normalise(float *image, int32_t planes, int32_t m, const float *facet_norm, void *stream);
+
+/* GiveModelTessel(ToGrid=True) for one facet (ClassImToGrid.py:138-264): crops the main model
+ * image float32 [batch][M][M] around (xc, yc), divides by norm_image [M][M], multiplies by
+ * sw_img [N][N] (image orientation), divides by sphe [N][N] (zero where sphe < 1e-3),
+ * transposes and flips, scales by (overs N)^2 and writes fftshift(DFT(ifftshift(.))) / N^2
+ * into grid_out complex64 [batch][N][N].  work: a [batch][N][N] complex64 scratch buffer. */
+int ddfg_image_to_grid(ddfg_fft_plan *plan, const float *image, int32_t m, const float *norm_image,
+                       const float *sw_img, const float *sphe, int32_t xc, int32_t yc, double overs, void *grid_out,
+                       void *work, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,163 @@
+"""Generates the golden fixtures under tests/golden/ by running the reference itself.
+
+Run in a container that has the reference checkout (read-only) and the reference gridder built
+by oracle/build_ref.sh:
+
+    python tests/golden/make_golden.py [/path/to/reference]
+
+The reference's Python modules are imported with stand-ins for the absent optional packages
+(pyfftw -> numpy.fft, SharedArray, numexpr); nothing here is used by the product.  Fixtures:
+
+  cf_golden.npz    ModCF.ClassWTermModified tables for two facet centres
+  bda_golden.npz   ClassSmearMapping block maps (mode 1 and mode 2) of a small observation,
+                   packed in collectSmearMapping's key order
+  grid_golden.npz  inputs and outputs of pyGridderWPol32 / pyDeGridderWPol on a small case
+                   (4 correlations, Stokes I, per-visibility Jones, BDA blocks, flags)
+  sw_golden.npz    ModFFTW.ConvolveGaussian of a facet mask (the spatial-weight smoothing)
+"""
+import os
+import sys
+import types
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+
+
+def _stub(name, **attrs):
+    m = types.ModuleType(name)
+    m.__dict__.update(attrs)
+    sys.modules[name] = m
+    return m
+
+
+def _numexpr_evaluate(expr, out=None, casting=None, local_dict=None):
+    """numexpr.evaluate on numpy: evaluates expr with the caller's local variables."""
+    ns = dict(sys._getframe(1).f_locals if local_dict is None else local_dict)
+    ns.update(exp=np.exp, sqrt=np.sqrt, sin=np.sin, cos=np.cos, abs=np.abs)
+    res = eval(expr, {"__builtins__": {}}, ns)
+    if out is not None:
+        out[...] = res
+        return out
+    return res
+
+
+def import_reference():
+    sys.path.insert(0, REF)
+    pf = _stub("pyfftw")
+    pfi = _stub("pyfftw.interfaces")
+    def _np_fft(fn):
+        # pyfftw's numpy interface takes extra planner keywords that numpy.fft does not
+        def call(*a, **kw):
+            for k in ("overwrite_input", "threads", "planner_effort", "auto_align_input", "auto_contiguous"):
+                kw.pop(k, None)
+            return fn(*a, **kw)
+        return call
+
+    pfn = _stub("pyfftw.interfaces.numpy_fft",
+                **{k: _np_fft(getattr(np.fft, k)) for k in dir(np.fft) if not k.startswith("_")})
+    pf.interfaces = pfi
+    pfi.numpy_fft = pfn
+    pfi.cache = _stub("pyfftw.interfaces.cache", enable=lambda: None, set_keepalive_time=lambda t: None)
+    pfi.scipy_fftpack = _stub("pyfftw.interfaces.scipy_fftpack")
+    _stub("SharedArray")
+    _stub("numexpr", evaluate=_numexpr_evaluate)
+    # the process pool imports a compiled helper module at import time; it is never called here
+    cb = _stub("DDFacet.cbuild")
+    cg = _stub("DDFacet.cbuild.Gridder")
+    cb.Gridder = cg
+    cg._pyArrays3x = _stub("DDFacet.cbuild.Gridder._pyArrays3x")
+    from DDFacet.Imager import ModCF  # noqa: F401
+    from DDFacet.Data import ClassSmearMapping  # noqa: F401
+    from DDFacet.ToolsDir import ModFFTW  # noqa: F401
+    return ModCF, ClassSmearMapping, ModFFTW
+
+
+class CFDict(dict):
+    def addSharedArray(self, name, shape, dtype):
+        self[name] = np.zeros(shape, dtype)
+        return self[name]
+
+
+def main():
+    ModCF, SM, ModFFTW = import_reference()
+    sys.path.insert(0, ROOT)
+    from ddfacet_b200 import synth
+
+    freqs = np.linspace(1.30e9, 1.45e9, 8)
+    # ---- CF tables
+    out = {}
+    for i, lm in enumerate([(0.0, 0.0), (0.02, -0.01)]):
+        w = ModCF.ClassWTermModified(Cell=3.0, Sup=7, Npix=129, Freqs=freqs, wmax=3000.0, Nw=4, OverS=11,
+                                     lmShift=lm, cf_dict=CFDict(), compute_cf=True)
+        out[f"f{i}_lm"] = np.array(lm)
+        out[f"f{i}_sups"] = np.array(w.Sups)
+        out[f"f{i}_cucv"] = np.array([w.Cu, w.Cv])
+        out[f"f{i}_ifzf"] = np.asarray(w.ifzfCF)
+        for k, (a, b) in enumerate(zip(w.Wplanes, w.WplanesConj)):
+            out[f"f{i}_w{k}"] = a
+            out[f"f{i}_wc{k}"] = b
+    out["freqs"] = freqs
+    np.savez_compressed(os.path.join(HERE, "cf_golden.npz"), **out)
+
+    # ---- BDA maps
+    obs = synth.make_observation(7, 7, 1500.0, 34.0, 40.0, 0.25, 30.0, 8, 1.30e9, 1.45e9)
+    chan_map = np.array([0, 0, 0, 0, 1, 1, 1, 1], np.int32)
+    dfreq = float(freqs[1] - freqs[0])
+    DATA = {"A0": obs.A0, "A1": obs.A1, "uvw": obs.uvw, "dfreqs": dfreq, "freqs": obs.freqs}
+    bda = {"A0": obs.A0, "A1": obs.A1, "uvw": obs.uvw, "freqs": obs.freqs, "chan_map": chan_map, "dfreq": dfreq}
+    for mode, fn in ((1, SM.GiveBlocksRowsListBL_old), (2, SM.GiveBlocksRowsListBL)):
+        for dphi_name, decorr in (("a", 0.02), ("b", 0.002)):
+            dPhi = np.sqrt(6. * (1. - (1. - decorr)))
+            l = 0.01
+            per = {}
+            for a0 in range(obs.nant):
+                for a1 in range(obs.nant):
+                    if a0 == a1:
+                        continue
+                    r = fn(a0, a1, DATA, dPhi, l, chan_map)
+                    if r[0] is not None:
+                        per["%d:%d" % (a0, a1)] = (np.array(r[0]), np.array(r[1]))
+            keys = sorted(per.keys())
+            nb = sum(len(per[k][1]) for k in keys)
+            body = np.concatenate([per[k][0] for k in keys]).astype(np.int32)
+            sizes = np.concatenate([per[k][1] for k in keys]).astype(np.int32)
+            m = np.concatenate([[nb, nb >> 32], sizes, body]).astype(np.int32)
+            bda[f"map_mode{mode}_{dphi_name}"] = m
+            bda[f"dphi_{dphi_name}"] = dPhi
+    bda["l"] = 0.01
+    np.savez_compressed(os.path.join(HERE, "bda_golden.npz"), **bda)
+
+    # ---- reference gridder / degridder on a small case
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import cases
+
+    c = cases.make_case(seed=21, nant=8, ntimes=12, nchan=8, ncorr=4, stokes_ids=(1,), npix=129, cell_arcsec=6.0,
+                        nw=3, bda_mode=1, dphi=np.sqrt(6 * 0.05), flag_frac=0.05, lm=(0.01, -0.004))
+    cases.add_jones(c, mode=1, nt=3, nd=2, idir=1)
+    r = cases.run_ref_grid(c)
+    vr = cases.run_ref_degrid(c, r["grid"], vis0=c.vis)
+    g = dict(vis=c.vis, uvw=c.uvw, flags=c.flags, weights=c.weights, freqs=c.freqs, chan_map=c.chan_map, bda=c.bda,
+             incr=c.incr, winfos=c.winfos, facet_infos=c.facet_infos, lm=np.array(c.lm),
+             jones_kms=c.jones["kms"], jones_tmap=c.jones["kms_tmap"], jones_cmap=c.jones["kms_cmap"],
+             A0=c.jones["A0"], A1=c.jones["A1"], idir=c.jones["idir_kms"],
+             grid=r["grid"], sumwt=r["sumwt"], sumjones=r["sumjones"], sumjones_chan=r["sumjones_chan"], vis_degrid=vr)
+    for k, (a, b) in enumerate(zip(c.wt.Wplanes, c.wt.WplanesConj)):
+        g[f"w{k}"] = a
+        g[f"wc{k}"] = b
+    g["nw"] = len(c.wt.Wplanes)
+    np.savez_compressed(os.path.join(HERE, "grid_golden.npz"), **g)
+
+    # ---- spatial-weight smoothing
+    mask = np.zeros((1, 1, 97, 97), np.float32)
+    mask[0, 0, 20:70, 25:80] = 1
+    sw = ModFFTW.ConvolveGaussian(shareddict={"in": mask, "out": mask.copy()}, field_in="in", field_out="out", ch=0,
+                                  CellSizeRad=1, GaussPars_ch=(10, 10, 0))
+    np.savez_compressed(os.path.join(HERE, "sw_golden.npz"), mask=mask[0, 0], sw=np.asarray(sw).reshape(97, 97))
+    print("golden fixtures written to", HERE)
+
+
+if __name__ == "__main__":
+    main()
