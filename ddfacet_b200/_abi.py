@@ -99,6 +99,7 @@ SIGNATURES = {
     "ddfg_fft_plan_create": (C.c_int, [_i32, _i32, C.POINTER(_vp)]),
     "ddfg_fft_plan_destroy": (C.c_int, [_vp]),
     "ddfg_grid_to_image": (C.c_int, [_vp, _vp, _f64, _vp, _vp]),
+    "ddfg_fft_centred": (C.c_int, [_vp, _vp, _i32, _f64, _vp, _vp]),
     "ddfg_stitch_facet": (C.c_int, [_vp, _i32, _i32, _i32, _vp, _vp, _vp, _vp, _vp, _i32, _i32, _i32, _vp]),
     "ddfg_image_normalise": (C.c_int, [_vp, _i32, _i32, _vp, _vp]),
     "ddfg_image_to_grid": (C.c_int, [_vp, _vp, _i32, _vp, _vp, _vp, _i32, _i32, _f64, _vp, _vp, _vp]),

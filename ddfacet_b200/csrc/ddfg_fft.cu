@@ -190,6 +190,23 @@ extern "C" int ddfg_grid_to_image(ddfg_fft_plan *p, void *grid, double scale, vo
   return DDFG_OK;
 }
 
+extern "C" int ddfg_fft_centred(ddfg_fft_plan *p, void *data, int32_t inverse, double scale, void *work,
+                                void *stream_) {
+  cudaStream_t stream = (cudaStream_t)stream_;
+  if (!p || !data || !work) return ddfg_set_error(DDFG_EINVAL, "fft_centred: null argument");
+  const int64_t total = (int64_t)p->batch * p->n * p->n;
+  ishift_scale_kernel<<<nctas_for(total), 256, 0, stream>>>((const float2 *)data, (float2 *)work, p->n, p->batch, 1.f);
+  if (cufftSetStream(p->h, stream) != CUFFT_SUCCESS) return ddfg_set_error(DDFG_ECUDA, "fft_centred: cufftSetStream");
+  if (cufftExecC2C(p->h, (cufftComplex *)work, (cufftComplex *)work, inverse ? CUFFT_INVERSE : CUFFT_FORWARD) !=
+      CUFFT_SUCCESS)
+    return ddfg_set_error(DDFG_ECUDA, "fft_centred: cufftExecC2C failed");
+  shift_scale_kernel<<<nctas_for(total), 256, 0, stream>>>((const float2 *)work, (float2 *)data, p->n, p->batch,
+                                                             (float)scale);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return ddfg_set_error(DDFG_ECUDA, "fft_centred: %s", cudaGetErrorString(e));
+  return DDFG_OK;
+}
+
 extern "C" int ddfg_stitch_facet(const void *dirty, int32_t nband, int32_t npol, int32_t n, const float *sphe,
                                  const float *invsphe, const float *sw_grid, const double *weights, float *image,
                                  int32_t m, int32_t xc, int32_t yc, void *stream_) {

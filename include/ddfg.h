@@ -214,6 +214,11 @@ int ddfg_fft_plan_destroy(ddfg_fft_plan *plan);
  * ifft2 times N^2); scale is OverS^2 for GridToIm.  work: a second [batch][N][N] buffer. */
 int ddfg_grid_to_image(ddfg_fft_plan *plan, void *grid, double scale, void *work, void *stream);
 
+/* data[batch][N][N] <- fftshift(DFT(ifftshift(data))) * scale, forward or (inverse != 0)
+ * unnormalised inverse DFT: ModFFTW.FFTW_2Donly.fft/ifft (ModFFTW.py:557-599) with scale 1/N^2
+ * (fft) or 1 (ifft times N^2).  work: a second [batch][N][N] buffer. */
+int ddfg_fft_centred(ddfg_fft_plan *plan, void *data, int32_t inverse, double scale, void *work, void *stream);
+
 /* Adds one facet's dirty image (complex64 [nband][npol][N][N] from ddfg_grid_to_image) into the
  * main image float32 [nband][npol][M][M] (FacetsToIm_Channel, ClassFacetMachine.py:1331-1410):
  * Re(dirty) * invsphe * sw_grid / weights[band][pol] (weights 0 counts as 1), zero where
