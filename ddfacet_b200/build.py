@@ -13,6 +13,7 @@ import os
 import shutil
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
@@ -49,12 +50,17 @@ def build(force: bool = False, verbose: bool = False, ptxas_verbose: bool = Fals
               "--expt-relaxed-constexpr"]
     if ptxas_verbose:
         common += ["-Xptxas", "-v"]
-    for src in SOURCES:
+    def compile_one(src):
         obj = os.path.join(LIBDIR, src.replace(".cu", ".o"))
         cmd = common + ["-c", os.path.join(CSRC, src), "-o", obj]
         if verbose:
             print(" ".join(cmd))
-        r = subprocess.run(cmd, capture_output=True, text=True)
+        return src, obj, subprocess.run(cmd, capture_output=True, text=True)
+
+    # one nvcc per translation unit, in parallel (each is single-threaded)
+    with ThreadPoolExecutor(max_workers=max(1, min(len(SOURCES), os.cpu_count() or 1))) as ex:
+        results = list(ex.map(compile_one, SOURCES))
+    for src, obj, r in results:
         if r.returncode != 0:
             raise RuntimeError(f"nvcc failed on {src}:\n{r.stderr}")
         if ptxas_verbose or verbose:

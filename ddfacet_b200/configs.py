@@ -44,8 +44,9 @@ class Workload:
     info: dict = field(default_factory=dict)
 
 
-def _gen_vis_gpu(uvw_d, freqs_d, l, m, s, ncorr, noise_sigma, seed, dev, row_chunk=1 << 16):
-    """Point-source visibilities + complex noise on the GPU (FP64 phase, complex64 result)."""
+def _gen_vis_gpu(uvw_d, freqs_d, l, m, s, ncorr, noise_sigma, seed, dev, row_chunk=1 << 14):
+    """Point-source visibilities + complex noise on the GPU (FP64 phase, complex64 result).
+    All sources of a row chunk in one pass, so generation takes a few thousand launches."""
     nrow = uvw_d.shape[0]
     nchan = freqs_d.numel()
     out = torch.empty((nrow, nchan, ncorr), dtype=torch.complex64, device=dev)
@@ -54,20 +55,21 @@ def _gen_vis_gpu(uvw_d, freqs_d, l, m, s, ncorr, noise_sigma, seed, dev, row_chu
     lt = torch.tensor(l, dtype=torch.float64, device=dev)
     mt = torch.tensor(m, dtype=torch.float64, device=dev)
     nt = torch.sqrt(1 - lt ** 2 - mt ** 2) - 1
+    lmn = torch.stack([lt, mt, nt])                                             # [3][nsrc]
     st = torch.tensor(s, dtype=torch.float32, device=dev)
     fr = (freqs_d / C_LIGHT).to(torch.float64)
     for r0 in range(0, nrow, row_chunk):
         uu = uvw_d[r0:r0 + row_chunk]
-        acc = torch.zeros((uu.shape[0], nchan), dtype=torch.complex64, device=dev)
-        for k in range(lt.numel()):
-            ph = uu[:, 0] * lt[k] + uu[:, 1] * mt[k] + uu[:, 2] * nt[k]          # metres
-            turns = ph[:, None] * fr[None, :]
-            frac = (turns - torch.round(turns)).to(torch.float32)
-            acc += st[k] * torch.polar(torch.ones_like(frac), 2 * np.pi * frac)
+        turns = (uu @ lmn)[:, :, None] * fr[None, None, :]                        # [rows][nsrc][nchan]
+        frac = (turns - torch.round(turns)).to(torch.float32)
+        del turns
+        acc = (torch.polar(st[None, :, None].expand_as(frac), 2 * np.pi * frac)).sum(dim=1)
+        del frac
         noise = torch.randn((uu.shape[0], nchan, ncorr, 2), generator=g, device=dev) * noise_sigma
         blk = torch.view_as_complex(noise.contiguous())
         blk[:, :, 0] += acc
-        blk[:, :, ncorr - 1] += acc
+        if ncorr > 1:
+            blk[:, :, ncorr - 1] += acc
         out[r0:r0 + row_chunk] = blk
     return out
 

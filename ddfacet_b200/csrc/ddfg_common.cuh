@@ -36,6 +36,13 @@ __device__ __forceinline__ float cabs2(float2 a) { return sqrtf(a.x * a.x + a.y 
 __device__ __forceinline__ float2 cmuli(float2 a) { return make_float2(-a.y, a.x); }  // a * i
 __device__ __forceinline__ float2 czero() { return make_float2(0.f, 0.f); }
 
+// grid[cell] += v as one vector reduction without a return value (red.global.add.v2.f32,
+// sm_90+): the same addition as atomicAdd(float2*), which is issued as a returning atomic, but
+// the issuing warp does not wait for the L2 round trip.
+__device__ __forceinline__ void red_add(float2 *p, float2 v) {
+  asm volatile("red.global.add.v2.f32 [%0], {%1, %2};" ::"l"(p), "f"(v.x), "f"(v.y) : "memory");
+}
+
 // 2x2 complex matrix, element order [0]=(0,0) [1]=(0,1) [2]=(1,0) [3]=(1,1) (JonesServer.h:38-81)
 struct M2 {
   float2 v[4];

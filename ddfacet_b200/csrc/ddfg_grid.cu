@@ -118,7 +118,7 @@ __global__ void __launch_bounds__(256) grid_kernel(const ddfg_vis vs, const ddfg
                 float2 *cell = grid + (j[r].base + lt.off[k]);
 #pragma unroll
                 for (int p = 0; p < NPOL; ++p)
-                  if (p < npol_used) atomicAdd(cell + (size_t)p * plane_sz, cmul(sv[r][p], c[r][k]));
+                  if (p < npol_used) red_add(cell + (size_t)p * plane_sz, cmul(sv[r][p], c[r][k]));
               }
             }
           }
@@ -132,7 +132,7 @@ __global__ void __launch_bounds__(256) grid_kernel(const ddfg_vis vs, const ddfg
               float2 *cell = grid + (j[r].base + sy * f.nx + (t - sy * Sr));
 #pragma unroll
               for (int p = 0; p < NPOL; ++p)
-                if (p < npol_used) atomicAdd(cell + (size_t)p * plane_sz, cmul(sv[r][p], cv));
+                if (p < npol_used) red_add(cell + (size_t)p * plane_sz, cmul(sv[r][p], cv));
             }
           }
         }

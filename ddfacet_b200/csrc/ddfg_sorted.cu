@@ -126,7 +126,7 @@ __device__ __forceinline__ void acc_flush(TapAcc<NPOL, SLOTS, COMP> &a, float2 *
             v.x += a.lo[k][p].x;
             v.y += a.lo[k][p].y;
           }
-          if (v.x != 0.f || v.y != 0.f) atomicAdd(cell + (size_t)p * plane_sz, v);
+          if (v.x != 0.f || v.y != 0.f) red_add(cell + (size_t)p * plane_sz, v);
         }
       }
     }
