@@ -222,19 +222,36 @@ struct JonesCache {
   }
 };
 
+// The row/channel indices a visibility's Jones lookup needs (antennas, time slots, Jones
+// channels), loaded once and reused for every facet of a launch.
+struct JonesIdx {
+  int a0, a1, tk, ck, tb, cb;
+};
+__device__ __forceinline__ JonesIdx jones_idx(const ddfg_jones &js, int64_t irow, int ichan) {
+  JonesIdx x;
+  x.a0 = js.a0[irow];
+  x.a1 = js.a1[irow];
+  x.tk = js.kms ? js.kms_tmap[irow] : 0;
+  x.ck = js.kms ? js.kms_cmap[ichan] : 0;
+  x.tb = js.beam ? js.beam_tmap[irow] : 0;
+  x.cb = js.beam ? js.beam_cmap[ichan] : 0;
+  return x;
+}
+
 // J0, J1 and BB of one visibility without a cache: what JonesCache::update computes after a
-// reset (every single-visibility block resets the reference's cache, gridder.h:184).
-__device__ __forceinline__ void jones_pair(const ddfg_jones &js, int idir_kms, int idir_beam, int64_t irow, int ichan,
-                                           double u, double v, M2 &j0, M2 &j1, float &bb) {
-  const int a0 = js.a0[irow], a1 = js.a1[irow];
+// reset (every single-visibility block resets the reference's cache, gridder.h:184), with the
+// indices already loaded.
+__device__ __forceinline__ void jones_pair_at(const ddfg_jones &js, int idir_kms, int idir_beam, const JonesIdx &x,
+                                              double u, double v, M2 &j0, M2 &j1, float &bb) {
+  const int a0 = x.a0, a1 = x.a1;
   M2 a = m2_unity(), b = m2_unity();
   if (js.beam) {
-    const int t = js.beam_tmap[irow], c = js.beam_cmap[ichan];
+    const int t = x.tb, c = x.cb;
     a = give_jones((const float2 *)js.beam, js.beam_dims, js.interp_coefs, t, a0, idir_beam, c, js.interp_mode);
     b = give_jones((const float2 *)js.beam, js.beam_dims, js.interp_coefs, t, a1, idir_beam, c, js.interp_mode);
   }
   if (js.kms) {
-    const int t = js.kms_tmap[irow], c = js.kms_cmap[ichan];
+    const int t = x.tk, c = x.ck;
     M2 k0 = give_jones((const float2 *)js.kms, js.kms_dims, js.interp_coefs, t, a0, idir_kms, c, js.interp_mode);
     M2 k1 = give_jones((const float2 *)js.kms, js.kms_dims, js.interp_coefs, t, a1, idir_kms, c, js.interp_mode);
     norm_jones(k0, js, u, v);
@@ -247,6 +264,12 @@ __device__ __forceinline__ void jones_pair(const ddfg_jones &js, int idir_kms, i
   j1 = b;
   const float t = (cabs2(a.v[0]) * cabs2(b.v[0]) + cabs2(a.v[3]) * cabs2(b.v[3])) * 0.5f;
   bb = t * t;
+}
+
+// The same, loading the indices of row irow and channel ichan.
+__device__ __forceinline__ void jones_pair(const ddfg_jones &js, int idir_kms, int idir_beam, int64_t irow, int ichan,
+                                           double u, double v, M2 &j0, M2 &j1, float &bb) {
+  jones_pair_at(js, idir_kms, idir_beam, jones_idx(js, irow, ichan), u, v, j0, j1, bb);
 }
 
 // ----------------------------------------------------------------------------------------
@@ -395,17 +418,19 @@ inline int tap_slots(int max_support) {
   return t <= 64 ? 2 : (t <= 128 ? 4 : 8);
 }
 
-// Per-lane tap offsets for the current support, recomputed only when the support changes:
+// Per-lane tap offsets for the current support and grid width, recomputed when either changes:
 // lane l owns taps t = l + 32 k (k < SLOTS), at cell offset (t / S) * nx + t % S.
 template <int SLOTS>
 struct LaneTaps {
-  int S;
+  int S, NX;
   int off[SLOTS];
-  __device__ __forceinline__ void reset() { S = -1; }
+  __device__ __forceinline__ void reset() { S = -1; NX = -1; }
+  // The offsets depend on the grid width too: facets of one launch may differ in size.
   __device__ __forceinline__ void set(int s_inv, int nx, int lane) {
     const int s = s_inv & 255;
-    if (s == S) return;
+    if (s == S && nx == NX) return;
     S = s;
+    NX = nx;
     const unsigned inv = (unsigned)s_inv >> 8;
 #pragma unroll
     for (int k = 0; k < SLOTS; ++k) {

@@ -24,6 +24,85 @@
 
 namespace ddfg {
 
+// Warp-cooperative tap scatter of the warp's 32 records onto facet f (gridder.h:353-362): each
+// record's footprint, CF offset and support travel in three shuffles; each lane keeps the cell
+// offsets of its taps for as long as the support and grid width stay the same.  Up to four
+// records of equal support are issued together so their CF loads are in flight at once.
+// Must be called by all 32 lanes.
+template <int NPOL, int SLOTS>
+__device__ __forceinline__ void scatter_records(const GridRecord<NPOL> &rec, const ddfg_facet &f, int npol_used,
+                                                LaneTaps<SLOTS> &lt, int lane) {
+  float2 *grid = (float2 *)f.grid;
+  const float2 *cfd = (const float2 *)f.cf_data;
+  const int plane_sz = f.nx * f.ny;
+  TapJob job;
+  if (rec.valid) job = tap_job(rec.g, rec.gridchan, f);
+  unsigned mask = __ballot_sync(0xffffffffu, rec.valid);
+  while (mask) {
+    int src[4];
+    int nr = 0;
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+      src[r] = mask ? __ffs(mask) - 1 : -1;
+      if (mask) {
+        mask &= mask - 1;
+        ++nr;
+      }
+    }
+    TapJob j[4];
+    float2 sv[4][NPOL];
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+      const int sr = src[r] >= 0 ? src[r] : src[0];
+      j[r] = shfl_job(job, sr);
+#pragma unroll
+      for (int p = 0; p < NPOL; ++p) {
+        sv[r][p].x = __shfl_sync(0xffffffffu, rec.stokes[p].x, sr);
+        sv[r][p].y = __shfl_sync(0xffffffffu, rec.stokes[p].y, sr);
+      }
+    }
+    const int S = j[0].s_inv & 255;
+    bool same = S * S <= 32 * SLOTS;
+#pragma unroll
+    for (int r = 1; r < 4; ++r) same = same && (r >= nr || (j[r].s_inv & 255) == S);
+    if (same) {
+      lt.set(j[0].s_inv, f.nx, lane);
+      float2 c[4][SLOTS];
+#pragma unroll
+      for (int r = 0; r < 4; ++r)
+#pragma unroll
+        for (int k = 0; k < SLOTS; ++k)
+          c[r][k] = (r < nr && lt.off[k] >= 0) ? __ldg(cfd + j[r].cfoff + lane + 32 * k) : czero();
+#pragma unroll
+      for (int r = 0; r < 4; ++r) {
+        if (r >= nr) break;
+#pragma unroll
+        for (int k = 0; k < SLOTS; ++k) {
+          if (lt.off[k] >= 0) {
+            float2 *cell = grid + (j[r].base + lt.off[k]);
+#pragma unroll
+            for (int p = 0; p < NPOL; ++p)
+              if (p < npol_used) red_add(cell + (size_t)p * plane_sz, cmul(sv[r][p], c[r][k]));
+          }
+        }
+      }
+    } else {
+      for (int r = 0; r < nr; ++r) {
+        const int Sr = j[r].s_inv & 255;
+        const unsigned inv = (unsigned)j[r].s_inv >> 8;
+        for (int t = lane; t < Sr * Sr; t += 32) {
+          const int sy = (int)(((unsigned)t * inv) >> 16);
+          const float2 cv = __ldg(cfd + j[r].cfoff + t);
+          float2 *cell = grid + (j[r].base + sy * f.nx + (t - sy * Sr));
+#pragma unroll
+          for (int p = 0; p < NPOL; ++p)
+            if (p < npol_used) red_add(cell + (size_t)p * plane_sz, cmul(sv[r][p], cv));
+        }
+      }
+    }
+  }
+}
+
 template <int NPOL, int SLOTS, bool SINGLE>
 __global__ void __launch_bounds__(256) grid_kernel(const ddfg_vis vs, const ddfg_jones js, const FacetPack pack,
                                                    const GridParams gp) {
@@ -49,9 +128,6 @@ __global__ void __launch_bounds__(256) grid_kernel(const ddfg_vis vs, const ddfg
     __syncthreads();
 
     const double n0m1 = sqrt(1. - f.l0 * f.l0 - f.m0 * f.m0) - 1.;
-    float2 *grid = (float2 *)f.grid;
-    const float2 *cfd = (const float2 *)f.cf_data;
-    const int plane_sz = f.nx * f.ny;
     JonesCache jc;
     LaneTaps<SLOTS> lt;
     lt.reset();
@@ -67,76 +143,7 @@ __global__ void __launch_bounds__(256) grid_kernel(const ddfg_vis vs, const ddfg
 
       warp_add_block_sums<NPOL, SINGLE>(vs, js, f, gp, b, rec, npol_used, s_sumwt, s_sumj, s_chan, jc);
 
-      // Warp-cooperative tap scatter of the 32 records (gridder.h:353-362): the record's
-      // footprint, CF offset and support travel in three shuffles; each lane keeps the cell
-      // offsets of its taps for as long as the support stays the same.  Up to four records of
-      // equal support are issued together so their CF loads are in flight at once.
-      TapJob job;
-      if (rec.valid) job = tap_job(rec.g, rec.gridchan, f);
-      unsigned mask = __ballot_sync(0xffffffffu, rec.valid);
-      while (mask) {
-        int src[4];
-        int nr = 0;
-#pragma unroll
-        for (int r = 0; r < 4; ++r) {
-          src[r] = mask ? __ffs(mask) - 1 : -1;
-          if (mask) {
-            mask &= mask - 1;
-            ++nr;
-          }
-        }
-        TapJob j[4];
-        float2 sv[4][NPOL];
-#pragma unroll
-        for (int r = 0; r < 4; ++r) {
-          const int sr = src[r] >= 0 ? src[r] : src[0];
-          j[r] = shfl_job(job, sr);
-#pragma unroll
-          for (int p = 0; p < NPOL; ++p) {
-            sv[r][p].x = __shfl_sync(0xffffffffu, rec.stokes[p].x, sr);
-            sv[r][p].y = __shfl_sync(0xffffffffu, rec.stokes[p].y, sr);
-          }
-        }
-        const int S = j[0].s_inv & 255;
-        bool same = S * S <= 32 * SLOTS;
-#pragma unroll
-        for (int r = 1; r < 4; ++r) same = same && (r >= nr || (j[r].s_inv & 255) == S);
-        if (same) {
-          lt.set(j[0].s_inv, f.nx, lane);
-          float2 c[4][SLOTS];
-#pragma unroll
-          for (int r = 0; r < 4; ++r)
-#pragma unroll
-            for (int k = 0; k < SLOTS; ++k)
-              c[r][k] = (r < nr && lt.off[k] >= 0) ? __ldg(cfd + j[r].cfoff + lane + 32 * k) : czero();
-#pragma unroll
-          for (int r = 0; r < 4; ++r) {
-            if (r >= nr) break;
-#pragma unroll
-            for (int k = 0; k < SLOTS; ++k) {
-              if (lt.off[k] >= 0) {
-                float2 *cell = grid + (j[r].base + lt.off[k]);
-#pragma unroll
-                for (int p = 0; p < NPOL; ++p)
-                  if (p < npol_used) red_add(cell + (size_t)p * plane_sz, cmul(sv[r][p], c[r][k]));
-              }
-            }
-          }
-        } else {
-          for (int r = 0; r < nr; ++r) {
-            const int Sr = j[r].s_inv & 255;
-            const unsigned inv = (unsigned)j[r].s_inv >> 8;
-            for (int t = lane; t < Sr * Sr; t += 32) {
-              const int sy = (int)(((unsigned)t * inv) >> 16);
-              const float2 cv = __ldg(cfd + j[r].cfoff + t);
-              float2 *cell = grid + (j[r].base + sy * f.nx + (t - sy * Sr));
-#pragma unroll
-              for (int p = 0; p < NPOL; ++p)
-                if (p < npol_used) red_add(cell + (size_t)p * plane_sz, cmul(sv[r][p], cv));
-            }
-          }
-        }
-      }
+      scatter_records<NPOL, SLOTS>(rec, f, npol_used, lt, lane);
     }
     __syncthreads();
     // Flush this CTA's sums for facet fi.
@@ -149,6 +156,70 @@ __global__ void __launch_bounds__(256) grid_kernel(const ddfg_vis vs, const ddfg
         if (f.sumjones_chan && s_chan[i] != 0.) atomicAdd(&f.sumjones_chan[i], s_chan[i]);
     }
     __syncthreads();
+  }
+}
+
+// Single-visibility blocks, facet-inner: each warp loads its 32 visibilities' facet-independent
+// inputs (map entries, uvw, flags, weights, visibilities, Jones indices) once and grids them onto
+// every facet of the launch in turn, instead of re-reading them once per facet.  Per-facet weight
+// and Jones sums have their own shared-memory accumulators (acc_stride doubles each).
+template <int NPOL, int SLOTS>
+__global__ void __launch_bounds__(256) grid_single_fi_kernel(const ddfg_vis vs, const ddfg_jones js,
+                                                             const FacetPack pack, const GridParams gp,
+                                                             int acc_stride) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  ddfg_facet *sf = (ddfg_facet *)smem_raw;
+  double *s_n0m1 = (double *)(sf + DDFG_FACETS_PER_LAUNCH);
+  double *s_acc = s_n0m1 + DDFG_FACETS_PER_LAUNCH;
+  stage_facets(pack, sf);
+  for (int i = threadIdx.x; i < pack.n * acc_stride; i += blockDim.x) s_acc[i] = 0.;
+  __syncthreads();
+  if (threadIdx.x < pack.n) {
+    const ddfg_facet &f = sf[threadIdx.x];
+    s_n0m1[threadIdx.x] = sqrt(1. - f.l0 * f.l0 - f.m0 * f.m0) - 1.;
+  }
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  const int warp = threadIdx.x >> 5;
+  const int nwarps = blockDim.x >> 5;
+  const int64_t nstripes = (vs.nblocks + 31) / 32;
+  JonesCache jc;  // not used by single-visibility blocks
+  LaneTaps<SLOTS> lt;
+  lt.reset();
+
+  for (int64_t s = (int64_t)blockIdx.x * nwarps + warp; s < nstripes; s += (int64_t)gridDim.x * nwarps) {
+    const int64_t b = s * 32 + lane;
+    SingleIn in;
+    in.valid = false;
+    if (b < vs.nblocks) load_single(vs, js, gp, b, in);
+    if (!__any_sync(0xffffffffu, in.valid)) continue;
+    for (int fi = 0; fi < pack.n; ++fi) {
+      const ddfg_facet &f = sf[fi];
+      const int npol_used = min(gp.nvispol, f.npol);
+      double *a = s_acc + (size_t)fi * acc_stride;
+      double *a_sumwt = a;                      // [nband][npol]
+      double *a_sumj = a + f.nband * f.npol;    // [2][nband]
+      double *a_chan = a_sumj + 2 * f.nband;    // [2][nchan]
+      GridRecord<NPOL> rec;
+      grid_single_facet<NPOL>(in, vs, js, f, gp, s_n0m1[fi], rec);
+      warp_add_block_sums<NPOL, true>(vs, js, f, gp, b, rec, npol_used, a_sumwt, a_sumj, a_chan, jc);
+      scatter_records<NPOL, SLOTS>(rec, f, npol_used, lt, lane);
+    }
+  }
+  __syncthreads();
+  // Flush this CTA's sums for every facet of the launch.
+  for (int fi = 0; fi < pack.n; ++fi) {
+    const ddfg_facet &f = sf[fi];
+    const double *a = s_acc + (size_t)fi * acc_stride;
+    const int nsw = f.nband * f.npol;
+    for (int i = threadIdx.x; i < nsw; i += blockDim.x)
+      if (f.sumwt && a[i] != 0.) atomicAdd(&f.sumwt[i], a[i]);
+    if (js.mode != 0) {
+      for (int i = threadIdx.x; i < 2 * f.nband; i += blockDim.x)
+        if (f.sumjones && a[nsw + i] != 0.) atomicAdd(&f.sumjones[i], a[nsw + i]);
+      for (int i = threadIdx.x; i < 2 * vs.nchan; i += blockDim.x)
+        if (f.sumjones_chan && a[nsw + 2 * f.nband + i] != 0.) atomicAdd(&f.sumjones_chan[i], a[nsw + 2 * f.nband + i]);
+    }
   }
 }
 
@@ -170,12 +241,38 @@ int ddfg_launch_grid(const ddfg_vis *vs, const ddfg_jones *js, const ddfg_facet 
   for (int i = 0; i < nfacets; ++i) max_band = max(max_band, facets[i].nband * (facets[i].npol + 2));
   const size_t smem = sizeof(ddfg_facet) * DDFG_FACETS_PER_LAUNCH + sizeof(double) * ((size_t)max_band + 2 * (size_t)vs->nchan);
   if (smem > 160 * 1024) return ddfg_set_error(DDFG_ESIZE, "grid: too many bands/channels for the shared accumulators");
+  // Facet-inner single-visibility kernel when every facet's accumulators fit in shared memory.
+  const int acc_stride = max_band + 2 * vs->nchan;
+  const size_t smem_fi = sizeof(ddfg_facet) * DDFG_FACETS_PER_LAUNCH + sizeof(double) * DDFG_FACETS_PER_LAUNCH +
+                         sizeof(double) * (size_t)DDFG_FACETS_PER_LAUNCH * (size_t)acc_stride;
+  const bool facet_inner = vs->single_vis_blocks && smem_fi <= 64 * 1024;
   for (int f0 = 0; f0 < nfacets; f0 += DDFG_FACETS_PER_LAUNCH) {
     FacetPack pack;
     pack.n = min(DDFG_FACETS_PER_LAUNCH, nfacets - f0);
     for (int i = 0; i < pack.n; ++i) pack.f[i] = facets[f0 + i];
     const int npol = nvispol;
     cudaError_t e;
+    if (facet_inner) {
+#define LAUNCH_F1(NP, SL)                                                                                          \
+  do {                                                                                                             \
+    if (smem_fi > 48 * 1024)                                                                                       \
+      cudaFuncSetAttribute(grid_single_fi_kernel<NP, SL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_fi); \
+    grid_single_fi_kernel<NP, SL><<<num_ctas, 256, smem_fi, stream>>>(*vs, *js, pack, gp, acc_stride);             \
+  } while (0)
+#define LAUNCH_F_NP(SL)              \
+  switch (npol) {                    \
+    case 1: LAUNCH_F1(1, SL); break; \
+    case 2: LAUNCH_F1(2, SL); break; \
+    case 3: LAUNCH_F1(3, SL); break; \
+    default: LAUNCH_F1(4, SL); break; \
+  }
+      if (slots == 2) { LAUNCH_F_NP(2) } else if (slots == 4) { LAUNCH_F_NP(4) } else { LAUNCH_F_NP(8) }
+#undef LAUNCH_F_NP
+#undef LAUNCH_F1
+      e = cudaGetLastError();
+      if (e != cudaSuccess) return ddfg_set_error(DDFG_ECUDA, "grid launch: %s", cudaGetErrorString(e));
+      continue;
+    }
 #define LAUNCH_G1(NP, SL, SG)                                                                                 \
   do {                                                                                                        \
     if (smem > 48 * 1024)                                                                                     \

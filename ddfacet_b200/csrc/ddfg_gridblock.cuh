@@ -30,14 +30,20 @@ struct GridRecord {
   bool single_chan;       // one channel: its channel sums are the block sums
 };
 
-// A block of exactly one row and one channel (every block of a map built without averaging):
-// the walk of gridder.h:184-351 with its loops, means and cache collapsed.  Sums over one term
-// equal that term exactly (0 + x == x, x / 1 == x), so the FP64 index inputs are the same.
-template <int NPOL>
-__device__ __forceinline__ void grid_single_record(const ddfg_vis &vs, const ddfg_jones &js, const ddfg_facet &f,
-                                                   const GridParams &gp, int64_t b, double n0m1,
-                                                   GridRecord<NPOL> &rec) {
-  rec.valid = false;
+// Facet-independent inputs of a single-visibility block (one row, one channel), loaded once
+// and shared by every facet of a launch.
+struct SingleIn {
+  bool valid;
+  int ch, gridchan;
+  int64_t irow;
+  double U, V, W, recip, nu, fw;
+  M2 vm;        // the visibilities (unused for the PSF)
+  JonesIdx jx;  // valid when js.mode != 0
+};
+
+__device__ __forceinline__ void load_single(const ddfg_vis &vs, const ddfg_jones &js, const GridParams &gp, int64_t b,
+                                            SingleIn &in) {
+  in.valid = false;
   if (vs.sparsification && !vs.sparsification[b]) return;
   const int64_t start = vs.block_start[b];
   const int ch = vs.bda_map[start];
@@ -45,46 +51,70 @@ __device__ __forceinline__ void grid_single_record(const ddfg_vis &vs, const ddf
   const int64_t doff = (irow * vs.nchan + ch) * (int64_t)vs.ncorr;
   if (vs.flags[doff]) return;
   const int gridchan = vs.chan_map[ch];
-  if (gridchan < 0 || gridchan >= f.nband) return;
-  const double U = vs.uvw[3 * irow], V = vs.uvw[3 * irow + 1], W = vs.uvw[3 * irow + 2];
+  if (gridchan < 0) return;
+  in.ch = ch;
+  in.irow = irow;
+  in.gridchan = gridchan;
+  in.U = vs.uvw[3 * irow];
+  in.V = vs.uvw[3 * irow + 1];
+  in.W = vs.uvw[3 * irow + 2];
+  in.recip = vs.recip_wvl ? vs.recip_wvl[ch] : vs.freqs[ch] / kC;
+  in.nu = vs.freqs[ch];
+  in.fw = (double)vs.weights[irow * vs.nchan + ch];
+  if (!gp.dopsf) {
+    const float2 *vp = (const float2 *)vs.vis + doff;
+    if (vs.ncorr == 4) {
+      const float4 a = *(const float4 *)vp, c = *(const float4 *)(vp + 2);
+      in.vm.v[0] = make_float2(a.x, a.y); in.vm.v[1] = make_float2(a.z, a.w);
+      in.vm.v[2] = make_float2(c.x, c.y); in.vm.v[3] = make_float2(c.z, c.w);
+    } else if (vs.ncorr == 2) {
+      in.vm.v[0] = vp[0]; in.vm.v[1] = czero(); in.vm.v[2] = czero(); in.vm.v[3] = vp[1];
+    } else {
+      in.vm.v[0] = vp[0]; in.vm.v[1] = czero(); in.vm.v[2] = czero(); in.vm.v[3] = vp[0];
+    }
+  }
+  if (js.mode != 0) in.jx = jones_idx(js, irow, ch);
+  in.valid = true;
+}
+
+// The facet-dependent part of a single-visibility block: the walk of gridder.h:184-351 with its
+// loops, means and cache collapsed.  Sums over one term equal that term exactly (0 + x == x,
+// x / 1 == x), so the FP64 index inputs are the same as the reference's.
+template <int NPOL>
+__device__ __forceinline__ void grid_single_facet(const SingleIn &in, const ddfg_vis &vs, const ddfg_jones &js,
+                                                  const ddfg_facet &f, const GridParams &gp, double n0m1,
+                                                  GridRecord<NPOL> &rec) {
+  rec.valid = false;
+  if (!in.valid || in.gridchan >= f.nband) return;
+  const double U = in.U, V = in.V, W = in.W;
   const double umean = dadd(U, dmul(W, f.cu));
   const double vmean = dadd(V, dmul(W, f.cv));
-  const double recip = vs.recip_wvl ? vs.recip_wvl[ch] : vs.freqs[ch] / kC;
-  if (!block_geometry(f, umean, vmean, W, recip, rec.g)) return;
+  if (!block_geometry(f, umean, vmean, W, in.recip, rec.g)) return;
 
-  const double nu = vs.freqs[ch];
-  const double dec = decorr_factor(vs, f, gp.freq_mean0, irow);
+  const double dec = decorr_factor(vs, f, gp.freq_mean0, in.irow);
   const float decf = (float)dec;
   M2 vm;
   if (gp.dopsf) {
     vm.v[0] = make_float2(decf, 0.f); vm.v[1] = czero(); vm.v[2] = czero(); vm.v[3] = make_float2(decf, 0.f);
   } else {
-    const float2 *vp = (const float2 *)vs.vis + doff;
-    if (vs.ncorr == 4) {
-      const float4 a = *(const float4 *)vp, c = *(const float4 *)(vp + 2);
-      vm.v[0] = make_float2(a.x, a.y); vm.v[1] = make_float2(a.z, a.w);
-      vm.v[2] = make_float2(c.x, c.y); vm.v[3] = make_float2(c.z, c.w);
-    } else if (vs.ncorr == 2) {
-      vm.v[0] = vp[0]; vm.v[1] = czero(); vm.v[2] = czero(); vm.v[3] = vp[1];
-    } else {
-      vm.v[0] = vp[0]; vm.v[1] = czero(); vm.v[2] = czero(); vm.v[3] = vp[0];
-    }
+    vm = in.vm;
   }
-  const double fw = (double)vs.weights[irow * vs.nchan + ch];
+  const double fw = in.fw;
   const double fwd = fw * dec * dec;
   double sumjones = 0.;
   if (js.mode != 0) {
     M2 j0, j1;
     float bb;
     // mode 1 normalises with the row's uvw, mode 2 with the block mean (gridder.h:236, 294)
-    jones_pair(js, f.idir_kms, f.idir_beam, irow, ch, js.mode == 1 ? U : umean, js.mode == 1 ? V : vmean, j0, j1, bb);
+    jones_pair_at(js, f.idir_kms, f.idir_beam, in.jx, js.mode == 1 ? U : umean, js.mode == 1 ? V : vmean, j0, j1,
+                  bb);
     // PSF: J0^H J0 J1^H J1 times the smearing factor in both modes (gridder.h:236-242, 295-297)
     if (gp.dopsf) vm = m2_scale(m2_times(m2_times(m2_herm(j0), m2_times(j0, m2_herm(j1))), j1), make_float2(decf, 0.f));
     else vm = m2_times(m2_times(m2_herm(j0), vm), j1);
     sumjones = (double)bb * fwd;
   }
   const float2 corr = gp.dopsf ? make_float2(1.f, 0.f)
-                               : phasor_turns(-nu * (U * f.l0 + V * f.m0 + W * n0m1) * kInvC);
+                               : phasor_turns(-in.nu * (U * f.l0 + V * f.m0 + W * n0m1) * kInvC);
   const float2 wgt = cscale(corr, (float)fw);
   M2 acc;
   acc.v[0] = cmul(vm.v[0], wgt);
@@ -96,12 +126,22 @@ __device__ __forceinline__ void grid_single_record(const ddfg_vis &vs, const ddf
 #pragma unroll
   for (int p = 0; p < NPOL; ++p) rec.stokes[p] = st[p];
   rec.valid = true;
-  rec.gridchan = gridchan;
+  rec.gridchan = in.gridchan;
   rec.weight = fw;
   rec.sumjones = sumjones;
   rec.sumsqw = fwd;
-  rec.ch0 = ch;
+  rec.ch0 = in.ch;
   rec.single_chan = true;
+}
+
+// A block of exactly one row and one channel (every block of a map built without averaging).
+template <int NPOL>
+__device__ __forceinline__ void grid_single_record(const ddfg_vis &vs, const ddfg_jones &js, const ddfg_facet &f,
+                                                   const GridParams &gp, int64_t b, double n0m1,
+                                                   GridRecord<NPOL> &rec) {
+  SingleIn in;
+  load_single(vs, js, gp, b, in);
+  grid_single_facet<NPOL>(in, vs, js, f, gp, n0m1, rec);
 }
 
 // Walk one block for one facet: gridder.h:184-351.

@@ -159,6 +159,33 @@ def test_multi_facet_call_matches_single_calls():
     assert cases.rel_rms(vis0 - got, vis0 - want) < TOL
 
 
+def test_uneven_facets_one_call():
+    """Facets of different grid sizes (and more than one launch's worth) in one grid and one
+    degrid call, each against the reference on that facet alone."""
+    from ddfacet_b200 import device as D
+    sizes = [255, 201, 311, 149] * 5  # 20 facets: two launches of facet descriptors
+    lms = [(0.004 * (i % 5) - 0.008, 0.003 * (i // 5) - 0.004) for i in range(len(sizes))]
+    cs = [cases.make_case(npix=n, lm=lm, nw=2, ncorr=4, stokes_ids=(1,), ntimes=10) for n, lm in zip(sizes, lms)]
+    for c in cs[1:]:
+        c.vis = cs[0].vis
+    objs = [cases._gpu_objs(c) for c in cs]
+    D.grid(objs[0][0], [o[1] for o in objs], D.make_pol(cs[0].corr_ids, [1]))
+    refs = [cases.run_ref_grid(c) for c in cs]
+    for o, r in zip(objs, refs):
+        g = o[1].grid.cpu().numpy()
+        assert cases.rel_rms(g, r["grid"]) < TOL
+        np.testing.assert_array_equal(g != 0, r["grid"] != 0)
+        np.testing.assert_allclose(o[1].sumwt.cpu().numpy(), r["sumwt"], rtol=1e-9)
+    vis0 = cs[0].vis
+    want = vis0.copy()
+    for c, r in zip(cs, refs):
+        want = want - (vis0 - cases.run_ref_degrid(c, r["grid"], vis0=vis0))
+    objs = [cases._gpu_objs(c, model_grid=r["grid"], vis=vis0) for c, r in zip(cs, refs)]
+    D.degrid(objs[0][0], [o[1] for o in objs], D.make_pol(cs[0].corr_ids, [1]))
+    got = objs[0][0].vis.cpu().numpy()
+    assert cases.rel_rms(vis0 - got, vis0 - want) < TOL
+
+
 def test_unsupported_combination_raises():
     c = cases.make_case(ncorr=2, corr_ids=[9, 12], stokes_ids=(3,), nw=3)
     with pytest.raises(ValueError, match="Cannot convert input correlations"):
