@@ -28,6 +28,110 @@ namespace ddfg {
 // lane j adds the 32 partials of block j (one pass instead of a butterfly per block).
 constexpr int kPartialBytesPerWarp = 32 * 32 * 8;
 
+// Cooperative gather of every valid record's taps on facet f (degridder.h:202-212): four
+// records of equal support at once, lanes on consecutive taps of a CF row; the sum of record r
+// ends in lane r's mine[].  For one Stokes plane the lane partials are reduced through the
+// warp's shared-memory tile wpart (one column per record); otherwise by butterflies.
+// Must be called by all 32 lanes.
+template <int NPOL, int SLOTS>
+__device__ __forceinline__ void gather_records(bool valid, const TapJob &job, const ddfg_facet &f,
+                                               LaneTaps<SLOTS> &lt, float2 *wpart, int lane, float2 *mine) {
+#pragma unroll
+  for (int p = 0; p < NPOL; ++p) mine[p] = czero();
+  const int plane_sz = f.nx * f.ny;
+  const float2 *grid = (const float2 *)f.grid;
+  const float2 *cfd = (const float2 *)f.cf_data;
+  const unsigned vmask = __ballot_sync(0xffffffffu, valid);
+  unsigned mask = vmask;
+  while (mask) {
+    // Up to four records of equal support at once: their CF and grid loads overlap.
+    int src[4];
+    int nr = 0;
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+      src[r] = mask ? __ffs(mask) - 1 : -1;
+      if (mask) {
+        mask &= mask - 1;
+        ++nr;
+      }
+    }
+    TapJob j[4];
+#pragma unroll
+    for (int r = 0; r < 4; ++r) j[r] = shfl_job(job, src[r] >= 0 ? src[r] : src[0]);
+    const int S = j[0].s_inv & 255;
+    bool same = S * S <= 32 * SLOTS;
+#pragma unroll
+    for (int r = 1; r < 4; ++r) same = same && (r >= nr || (j[r].s_inv & 255) == S);
+    float2 acc[4][NPOL];
+#pragma unroll
+    for (int r = 0; r < 4; ++r)
+#pragma unroll
+      for (int p = 0; p < NPOL; ++p) acc[r][p] = czero();
+    if (same) {
+      lt.set(j[0].s_inv, f.nx, lane);
+      float2 c[4][SLOTS], gv[4][SLOTS][NPOL];
+#pragma unroll
+      for (int r = 0; r < 4; ++r)
+#pragma unroll
+        for (int k = 0; k < SLOTS; ++k) {
+          const bool on = r < nr && lt.off[k] >= 0;
+          c[r][k] = on ? __ldg(cfd + j[r].cfoff + lane + 32 * k) : czero();
+#pragma unroll
+          for (int p = 0; p < NPOL; ++p)
+            gv[r][k][p] = on ? __ldg(grid + (j[r].base + lt.off[k]) + (size_t)p * plane_sz) : czero();
+        }
+#pragma unroll
+      for (int r = 0; r < 4; ++r)
+#pragma unroll
+        for (int k = 0; k < SLOTS; ++k)
+#pragma unroll
+          for (int p = 0; p < NPOL; ++p) acc[r][p] = cadd(acc[r][p], cmul(gv[r][k][p], c[r][k]));
+    } else {
+      for (int r = 0; r < nr; ++r) {
+        const int Sr = j[r].s_inv & 255;
+        const unsigned inv = (unsigned)j[r].s_inv >> 8;
+        for (int t = lane; t < Sr * Sr; t += 32) {
+          const int sy = (int)(((unsigned)t * inv) >> 16);
+          const float2 cv = __ldg(cfd + j[r].cfoff + t);
+          const float2 *cell = grid + (j[r].base + sy * f.nx + (t - sy * Sr));
+#pragma unroll
+          for (int p = 0; p < NPOL; ++p) acc[r][p] = cadd(acc[r][p], cmul(__ldg(cell + (size_t)p * plane_sz), cv));
+        }
+      }
+    }
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+      if (r >= nr) break;
+      if (NPOL == 1) {
+        wpart[src[r] * 32 + lane] = acc[r][0];
+      } else {
+#pragma unroll
+        for (int p = 0; p < NPOL; ++p) {
+#pragma unroll
+          for (int o = 16; o > 0; o >>= 1) {
+            acc[r][p].x += __shfl_xor_sync(0xffffffffu, acc[r][p].x, o);
+            acc[r][p].y += __shfl_xor_sync(0xffffffffu, acc[r][p].y, o);
+          }
+        }
+        if (lane == src[r]) {
+#pragma unroll
+          for (int p = 0; p < NPOL; ++p) mine[p] = acc[r][p];
+        }
+      }
+    }
+  }
+  if (NPOL == 1) {
+    __syncwarp();
+    if (valid) {
+      float2 t = czero();
+#pragma unroll 8
+      for (int i = 0; i < 32; ++i) t = cadd(t, wpart[lane * 32 + ((i + lane) & 31)]);
+      mine[0] = t;
+    }
+    __syncwarp();
+  }
+}
+
 template <int NPOL, int SLOTS, bool SINGLE>
 __global__ void __launch_bounds__(256) degrid_kernel(const ddfg_vis vs, const ddfg_jones js,
                                                         const FacetPackD pack, const DegridParams dp) {
@@ -60,105 +164,79 @@ __global__ void __launch_bounds__(256) degrid_kernel(const ddfg_vis vs, const dd
       TapJob job;
       if (valid) job = tap_job(g, SINGLE ? sgc : d.gridchan, f);
 
-      // Cooperative gather of every valid block's taps (degridder.h:202-212).
       float2 mine[NPOL];
-#pragma unroll
-      for (int p = 0; p < NPOL; ++p) mine[p] = czero();
-      const int plane_sz = f.nx * f.ny;
-      const float2 *grid = (const float2 *)f.grid;
-      const float2 *cfd = (const float2 *)f.cf_data;
-      const unsigned vmask = __ballot_sync(0xffffffffu, valid);
-      unsigned mask = vmask;
-      while (mask) {
-        // Up to four records of equal support at once: their CF and grid loads overlap.
-        int src[4];
-        int nr = 0;
-#pragma unroll
-        for (int r = 0; r < 4; ++r) {
-          src[r] = mask ? __ffs(mask) - 1 : -1;
-          if (mask) {
-            mask &= mask - 1;
-            ++nr;
-          }
-        }
-        TapJob j[4];
-#pragma unroll
-        for (int r = 0; r < 4; ++r) j[r] = shfl_job(job, src[r] >= 0 ? src[r] : src[0]);
-        const int S = j[0].s_inv & 255;
-        bool same = S * S <= 32 * SLOTS;
-#pragma unroll
-        for (int r = 1; r < 4; ++r) same = same && (r >= nr || (j[r].s_inv & 255) == S);
-        float2 acc[4][NPOL];
-#pragma unroll
-        for (int r = 0; r < 4; ++r)
-#pragma unroll
-          for (int p = 0; p < NPOL; ++p) acc[r][p] = czero();
-        if (same) {
-          lt.set(j[0].s_inv, f.nx, lane);
-          float2 c[4][SLOTS], gv[4][SLOTS][NPOL];
-#pragma unroll
-          for (int r = 0; r < 4; ++r)
-#pragma unroll
-            for (int k = 0; k < SLOTS; ++k) {
-              const bool on = r < nr && lt.off[k] >= 0;
-              c[r][k] = on ? __ldg(cfd + j[r].cfoff + lane + 32 * k) : czero();
-#pragma unroll
-              for (int p = 0; p < NPOL; ++p)
-                gv[r][k][p] = on ? __ldg(grid + (j[r].base + lt.off[k]) + (size_t)p * plane_sz) : czero();
-            }
-#pragma unroll
-          for (int r = 0; r < 4; ++r)
-#pragma unroll
-            for (int k = 0; k < SLOTS; ++k)
-#pragma unroll
-              for (int p = 0; p < NPOL; ++p) acc[r][p] = cadd(acc[r][p], cmul(gv[r][k][p], c[r][k]));
-        } else {
-          for (int r = 0; r < nr; ++r) {
-            const int Sr = j[r].s_inv & 255;
-            const unsigned inv = (unsigned)j[r].s_inv >> 8;
-            for (int t = lane; t < Sr * Sr; t += 32) {
-              const int sy = (int)(((unsigned)t * inv) >> 16);
-              const float2 cv = __ldg(cfd + j[r].cfoff + t);
-              const float2 *cell = grid + (j[r].base + sy * f.nx + (t - sy * Sr));
-#pragma unroll
-              for (int p = 0; p < NPOL; ++p) acc[r][p] = cadd(acc[r][p], cmul(__ldg(cell + (size_t)p * plane_sz), cv));
-            }
-          }
-        }
-#pragma unroll
-        for (int r = 0; r < 4; ++r) {
-          if (r >= nr) break;
-          if (NPOL == 1) {
-            wpart[src[r] * 32 + lane] = acc[r][0];
-          } else {
-#pragma unroll
-            for (int p = 0; p < NPOL; ++p) {
-#pragma unroll
-              for (int o = 16; o > 0; o >>= 1) {
-                acc[r][p].x += __shfl_xor_sync(0xffffffffu, acc[r][p].x, o);
-                acc[r][p].y += __shfl_xor_sync(0xffffffffu, acc[r][p].y, o);
-              }
-            }
-            if (lane == src[r]) {
-#pragma unroll
-              for (int p = 0; p < NPOL; ++p) mine[p] = acc[r][p];
-            }
-          }
-        }
-      }
-      if (NPOL == 1) {
-        __syncwarp();
-        if (valid) {
-          float2 t = czero();
-#pragma unroll 8
-          for (int i = 0; i < 32; ++i) t = cadd(t, wpart[lane * 32 + ((i + lane) & 31)]);
-          mine[0] = t;
-        }
-        __syncwarp();
-      }
+      gather_records<NPOL, SLOTS>(valid, job, f, lt, wpart, lane, mine);
       if (valid) {
         if (SINGLE) degrid_single_apply<NPOL>(vs, js, f, dp, sch, srow, mine);
         else degrid_block_apply<NPOL>(vs, js, f, dp, d, mine);
+      }
+    }
+  }
+}
+
+// Single-visibility blocks: the warp loads its 32 visibilities' facet-independent inputs once,
+// sums the predictions of every facet of the launch in registers, and subtracts the sum from
+// each visibility once (one read-modify-write per launch instead of one per facet).
+template <int NPOL, int SLOTS>
+__global__ void __launch_bounds__(256, SLOTS == 2 ? 2 : 1) degrid_single_fi_kernel(const ddfg_vis vs, const ddfg_jones js,
+                                                               const FacetPackD pack, const DegridParams dp) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  ddfg_facet *sf = (ddfg_facet *)smem_raw;
+  double *s_n0m1 = (double *)(sf + DDFG_FACETS_PER_LAUNCH);
+  float2 *partial = (float2 *)(s_n0m1 + DDFG_FACETS_PER_LAUNCH);
+  stage_facets(pack, sf);
+  __syncthreads();
+  if (threadIdx.x < pack.n) {
+    const ddfg_facet &f = sf[threadIdx.x];
+    s_n0m1[threadIdx.x] = sqrt(1. - f.l0 * f.l0 - f.m0 * f.m0) - 1.;
+  }
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  const int warp = threadIdx.x >> 5;
+  const int nwarps = blockDim.x >> 5;
+  const int64_t nstripes = (vs.nblocks + 31) / 32;
+  float2 *wpart = partial + warp * 32 * 32;  // [block][lane], NPOL == 1 only
+  LaneTaps<SLOTS> lt;
+  lt.reset();
+
+  for (int64_t s = (int64_t)blockIdx.x * nwarps + warp; s < nstripes; s += (int64_t)gridDim.x * nwarps) {
+    const int64_t b = s * 32 + lane;
+    DSingleIn in;
+    in.valid = false;
+    if (b < vs.nblocks) degrid_load_single(vs, js, b, in);
+    if (!__any_sync(0xffffffffu, in.valid)) continue;
+    M2 sum;
+#pragma unroll
+    for (int p = 0; p < 4; ++p) sum.v[p] = czero();
+    bool any = false;
+    for (int fi = 0; fi < pack.n; ++fi) {
+      const ddfg_facet &f = sf[fi];
+      BlockGeom g;
+      const bool valid = degrid_single_geom_in(in, f, g);
+      TapJob job;
+      if (valid) job = tap_job(g, in.gridchan, f);
+      float2 mine[NPOL];
+      gather_records<NPOL, SLOTS>(valid, job, f, lt, wpart, lane, mine);
+      if (valid) {
+        const M2 vb = degrid_single_pred<NPOL>(in, vs, js, f, dp, s_n0m1[fi], mine);
+#pragma unroll
+        for (int p = 0; p < 4; ++p) sum.v[p] = cadd(sum.v[p], vb.v[p]);
+        any = true;
+      }
+    }
+    if (any) {
+      float2 *vp = (float2 *)vs.vis + (in.irow * vs.nchan + in.ch) * (int64_t)vs.ncorr;
+      if (vs.ncorr == 4) {
+        float4 a = *(float4 *)vp, c = *(float4 *)(vp + 2);
+        a.x -= sum.v[0].x; a.y -= sum.v[0].y; a.z -= sum.v[1].x; a.w -= sum.v[1].y;
+        c.x -= sum.v[2].x; c.y -= sum.v[2].y; c.z -= sum.v[3].x; c.w -= sum.v[3].y;
+        *(float4 *)vp = a;
+        *(float4 *)(vp + 2) = c;
+      } else if (vs.ncorr == 2) {
+        vp[0] = csub(vp[0], sum.v[0]);
+        vp[1] = csub(vp[1], sum.v[3]);
+      } else {
+        vp[0] = csub(vp[0], sum.v[0]);
       }
     }
   }
@@ -181,15 +259,22 @@ int ddfg_launch_degrid(const ddfg_vis *vs, const ddfg_jones *js, const ddfg_face
     pack.n = min(DDFG_FACETS_PER_LAUNCH, nfacets - f0);
     for (int i = 0; i < pack.n; ++i) pack.f[i] = facets[f0 + i];
     const size_t smem = sizeof(ddfg_facet) * DDFG_FACETS_PER_LAUNCH + (nvispol == 1 ? 8 * kPartialBytesPerWarp : 0);
-#define LAUNCH_D1(NP, SL, SG)                                                                                  \
-  do {                                                                                                         \
-    cudaFuncSetAttribute(degrid_kernel<NP, SL, SG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);   \
-    degrid_kernel<NP, SL, SG><<<num_ctas, 256, smem, stream>>>(*vs, *js, pack, dp);                            \
+    const size_t smem_fi = smem + sizeof(double) * DDFG_FACETS_PER_LAUNCH;
+#define LAUNCH_D1(NP, SL)                                                                                          \
+  do {                                                                                                             \
+    cudaFuncSetAttribute(degrid_kernel<NP, SL, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);    \
+    degrid_kernel<NP, SL, false><<<num_ctas, 256, smem, stream>>>(*vs, *js, pack, dp);                             \
   } while (0)
-#define LAUNCH_D(NP, SL)                                 \
-  do {                                                   \
-    if (vs->single_vis_blocks) LAUNCH_D1(NP, SL, true);  \
-    else LAUNCH_D1(NP, SL, false);                       \
+#define LAUNCH_DS(NP, SL)                                                                                          \
+  do {                                                                                                             \
+    cudaFuncSetAttribute(degrid_single_fi_kernel<NP, SL>, cudaFuncAttributeMaxDynamicSharedMemorySize,             \
+                         (int)smem_fi);                                                                            \
+    degrid_single_fi_kernel<NP, SL><<<num_ctas, 256, smem_fi, stream>>>(*vs, *js, pack, dp);                       \
+  } while (0)
+#define LAUNCH_D(NP, SL)                              \
+  do {                                                \
+    if (vs->single_vis_blocks) LAUNCH_DS(NP, SL);     \
+    else LAUNCH_D1(NP, SL);                           \
   } while (0)
 #define LAUNCH_D_NP(SL)             \
   switch (nvispol) {                \
@@ -201,6 +286,7 @@ int ddfg_launch_degrid(const ddfg_vis *vs, const ddfg_jones *js, const ddfg_face
     if (slots == 2) { LAUNCH_D_NP(2) } else if (slots == 4) { LAUNCH_D_NP(4) } else { LAUNCH_D_NP(8) }
 #undef LAUNCH_D_NP
 #undef LAUNCH_D
+#undef LAUNCH_DS
 #undef LAUNCH_D1
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return ddfg_set_error(DDFG_ECUDA, "degrid launch: %s", cudaGetErrorString(e));

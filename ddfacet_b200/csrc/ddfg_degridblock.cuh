@@ -126,6 +126,61 @@ __device__ __forceinline__ bool degrid_single_geom(const ddfg_vis &vs, const ddf
   return block_geometry(f, um, vm, W, rw, g);
 }
 
+// Facet-independent inputs of a single-visibility block for the degridder, loaded once and
+// shared by every facet of a launch.
+struct DSingleIn {
+  bool valid;
+  int ch, gridchan;
+  int64_t irow;
+  double U, V, W, recip, nu;
+  JonesIdx jx;  // valid when js.mode != 0
+};
+
+__device__ __forceinline__ void degrid_load_single(const ddfg_vis &vs, const ddfg_jones &js, int64_t b,
+                                                   DSingleIn &in) {
+  const int64_t start = vs.block_start[b];
+  in.ch = vs.bda_map[start];
+  in.irow = vs.bda_map[start + 2];
+  in.gridchan = vs.chan_map[in.ch];
+  in.valid = in.gridchan >= 0;
+  const double *up = vs.uvw + 3 * in.irow;
+  in.U = up[0];
+  in.V = up[1];
+  in.W = up[2];
+  in.recip = vs.recip_wvl ? vs.recip_wvl[in.ch] : vs.freqs[in.ch] / kC;
+  in.nu = vs.freqs[in.ch];
+  if (js.mode != 0) in.jx = jones_idx(js, in.irow, in.ch);
+}
+
+// degrid_single_geom from preloaded inputs.
+__device__ __forceinline__ bool degrid_single_geom_in(const DSingleIn &in, const ddfg_facet &f, BlockGeom &g) {
+  if (!in.valid || in.gridchan >= f.nband) return false;
+  const double um = dadd(in.U, dmul(in.W, f.cu));
+  const double vm = dadd(in.V, dmul(in.W, f.cv));
+  return block_geometry(f, um, vm, in.W, in.recip, g);
+}
+
+// The prediction of facet f for a single visibility (what degrid_single_apply subtracts):
+// Stokes -> correlations, J0 M J1^H, phasor exp(+i nu angle) and smearing (degridder.h:214-261).
+template <int NPOL>
+__device__ __forceinline__ M2 degrid_single_pred(const DSingleIn &in, const ddfg_vis &vs, const ddfg_jones &js,
+                                                 const ddfg_facet &f, const DegridParams &dp, double n0m1,
+                                                 const float2 *pred) {
+  float2 s[4];
+#pragma unroll
+  for (int p = 0; p < 4; ++p) s[p] = (p < NPOL) ? pred[p] : czero();
+  M2 cv = corr_from_stokes(dp.policy, s);
+  if (js.mode != 0) {
+    M2 j0, j1;
+    float bb;
+    jones_pair_at(js, f.idir_kms, f.idir_beam, in.jx, in.U, in.V, j0, j1, bb);
+    cv = m2_times(m2_times(j0, cv), m2_herm(j1));
+  }
+  const float dec = (float)decorr_factor(vs, f, in.nu, in.irow);
+  const float2 ph = cscale(phasor_turns(in.nu * (in.U * f.l0 + in.V * f.m0 + in.W * n0m1) * kInvC), dec);
+  return m2_scale(cv, ph);
+}
+
 template <int NPOL>
 __device__ __forceinline__ void degrid_single_apply(const ddfg_vis &vs, const ddfg_jones &js, const ddfg_facet &f,
                                                     const DegridParams &dp, int ch, int64_t irow, const float2 *pred) {

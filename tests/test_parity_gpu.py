@@ -176,10 +176,12 @@ def test_uneven_facets_one_call():
         assert cases.rel_rms(g, r["grid"]) < TOL
         np.testing.assert_array_equal(g != 0, r["grid"] != 0)
         np.testing.assert_allclose(o[1].sumwt.cpu().numpy(), r["sumwt"], rtol=1e-9)
-    vis0 = cs[0].vis
+    # degrid into zeros, so the comparison sees the predictions themselves rather than their
+    # small difference from the visibilities (whose float32 rounding would dominate)
+    vis0 = np.zeros_like(cs[0].vis)
     want = vis0.copy()
     for c, r in zip(cs, refs):
-        want = want - (vis0 - cases.run_ref_degrid(c, r["grid"], vis0=vis0))
+        want = want + cases.run_ref_degrid(c, r["grid"], vis0=vis0)
     objs = [cases._gpu_objs(c, model_grid=r["grid"], vis=vis0) for c, r in zip(cs, refs)]
     D.degrid(objs[0][0], [o[1] for o in objs], D.make_pol(cs[0].corr_ids, [1]))
     got = objs[0][0].vis.cpu().numpy()
