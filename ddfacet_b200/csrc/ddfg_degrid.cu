@@ -43,6 +43,79 @@ __device__ __forceinline__ void gather_records(bool valid, const TapJob &job, co
   const float2 *cfd = (const float2 *)f.cf_data;
   const unsigned vmask = __ballot_sync(0xffffffffu, valid);
   unsigned mask = vmask;
+  // Fast path: every valid record has the same support, which fits the slots: the lane's tap
+  // pointers are formed once; each record costs two shuffles and its CF and model loads.
+  const int first = mask ? __ffs(mask) - 1 : 0;
+  const int s_inv0 = __shfl_sync(0xffffffffu, valid ? job.s_inv : 0, first);
+  const int S0 = s_inv0 & 255;
+  if (mask && S0 * S0 <= 32 * SLOTS && __all_sync(0xffffffffu, !valid || (job.s_inv & 255) == S0)) {
+    lt.set(s_inv0, f.nx, lane);
+    const float2 *cf_lane = cfd + lane;
+    const float2 *g_lane[SLOTS];
+    bool on[SLOTS];
+#pragma unroll
+    for (int k = 0; k < SLOTS; ++k) {
+      on[k] = lt.off[k] >= 0;
+      g_lane[k] = grid + (on[k] ? lt.off[k] : 0);
+    }
+    while (mask) {
+      int src[4];
+      int nr = 0;
+#pragma unroll
+      for (int r = 0; r < 4; ++r) {
+        src[r] = mask ? __ffs(mask) - 1 : src[0];
+        if (mask) {
+          mask &= mask - 1;
+          ++nr;
+        }
+      }
+      int base[4], cfo[4];
+#pragma unroll
+      for (int r = 0; r < 4; ++r) {
+        base[r] = __shfl_sync(0xffffffffu, job.base, src[r]);
+        cfo[r] = __shfl_sync(0xffffffffu, job.cfoff, src[r]);
+      }
+      float2 c[4][SLOTS], gv[4][SLOTS][NPOL];
+#pragma unroll
+      for (int r = 0; r < 4; ++r)
+#pragma unroll
+        for (int k = 0; k < SLOTS; ++k) {
+          c[r][k] = on[k] ? __ldg(cf_lane + cfo[r] + 32 * k) : czero();
+#pragma unroll
+          for (int p = 0; p < NPOL; ++p)
+            gv[r][k][p] = on[k] ? __ldg(g_lane[k] + base[r] + (size_t)p * plane_sz) : czero();
+        }
+      float2 acc[4][NPOL];
+#pragma unroll
+      for (int r = 0; r < 4; ++r)
+#pragma unroll
+        for (int p = 0; p < NPOL; ++p) {
+          acc[r][p] = czero();
+#pragma unroll
+          for (int k = 0; k < SLOTS; ++k) acc[r][p] = cadd(acc[r][p], cmul(gv[r][k][p], c[r][k]));
+        }
+#pragma unroll
+      for (int r = 0; r < 4; ++r) {
+        if (r >= nr) break;
+        if (NPOL == 1) {
+          wpart[src[r] * 32 + lane] = acc[r][0];
+        } else {
+#pragma unroll
+          for (int p = 0; p < NPOL; ++p) {
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+              acc[r][p].x += __shfl_xor_sync(0xffffffffu, acc[r][p].x, o);
+              acc[r][p].y += __shfl_xor_sync(0xffffffffu, acc[r][p].y, o);
+            }
+          }
+          if (lane == src[r]) {
+#pragma unroll
+            for (int p = 0; p < NPOL; ++p) mine[p] = acc[r][p];
+          }
+        }
+      }
+    }
+  }
   while (mask) {
     // Up to four records of equal support at once: their CF and grid loads overlap.
     int src[4];

@@ -38,6 +38,68 @@ __device__ __forceinline__ void scatter_records(const GridRecord<NPOL> &rec, con
   TapJob job;
   if (rec.valid) job = tap_job(rec.g, rec.gridchan, f);
   unsigned mask = __ballot_sync(0xffffffffu, rec.valid);
+  if (!mask) return;
+  // Fast path: every valid record of the stripe has the same support, which fits the slots (the
+  // usual case: a stripe is one row's channels, all on one W plane).  The lane's tap pointers
+  // are formed once, and each record costs three shuffles, its CF loads and the reductions.
+  const int first = __ffs(mask) - 1;
+  const int s_inv0 = __shfl_sync(0xffffffffu, rec.valid ? job.s_inv : 0, first);
+  const int S0 = s_inv0 & 255;
+  if (S0 * S0 <= 32 * SLOTS && __all_sync(0xffffffffu, !rec.valid || (job.s_inv & 255) == S0)) {
+    lt.set(s_inv0, f.nx, lane);
+    const float2 *cf_lane = cfd + lane;
+    float2 *g_lane[SLOTS];
+    bool on[SLOTS];
+#pragma unroll
+    for (int k = 0; k < SLOTS; ++k) {
+      on[k] = lt.off[k] >= 0;
+      g_lane[k] = grid + (on[k] ? lt.off[k] : 0);
+    }
+    while (mask) {
+      int src[4];
+      int nr = 0;
+#pragma unroll
+      for (int r = 0; r < 4; ++r) {
+        src[r] = mask ? __ffs(mask) - 1 : src[0];
+        if (mask) {
+          mask &= mask - 1;
+          ++nr;
+        }
+      }
+      int base[4], cfo[4];
+      float2 sv[4][NPOL];
+#pragma unroll
+      for (int r = 0; r < 4; ++r) {
+        base[r] = __shfl_sync(0xffffffffu, job.base, src[r]);
+        cfo[r] = __shfl_sync(0xffffffffu, job.cfoff, src[r]);
+#pragma unroll
+        for (int p = 0; p < NPOL; ++p) {
+          sv[r][p].x = __shfl_sync(0xffffffffu, rec.stokes[p].x, src[r]);
+          sv[r][p].y = __shfl_sync(0xffffffffu, rec.stokes[p].y, src[r]);
+        }
+      }
+      float2 c[4][SLOTS];
+#pragma unroll
+      for (int r = 0; r < 4; ++r)
+#pragma unroll
+        for (int k = 0; k < SLOTS; ++k) c[r][k] = on[k] ? __ldg(cf_lane + cfo[r] + 32 * k) : czero();
+#pragma unroll
+      for (int r = 0; r < 4; ++r) {
+        if (r < nr) {
+#pragma unroll
+          for (int k = 0; k < SLOTS; ++k) {
+            if (on[k]) {
+              float2 *cell = g_lane[k] + base[r];
+#pragma unroll
+              for (int p = 0; p < NPOL; ++p)
+                if (NPOL == 1 || p < npol_used) red_add(cell + (size_t)p * plane_sz, cmul(sv[r][p], c[r][k]));
+            }
+          }
+        }
+      }
+    }
+    return;
+  }
   while (mask) {
     int src[4];
     int nr = 0;
