@@ -373,7 +373,12 @@ def run_gpu(args):
         "facets_per_launch": fpl,
         "roofline": {
             "bound": "hbm", "kernel": dom, "achieved": round(achieved, 2), "peak": hbm_peak, "unit": "GB/s",
-            "frac": round(achieved / hbm_peak, 5), "peak_kind": peak_kind, "traffic": None,
+            "frac": round(achieved / hbm_peak, 5), "peak_kind": peak_kind,
+            # DRAM bytes (read + write) of one 16-facet launch of the dominant kernel: 95.0 B per
+            # visibility (grid) / 113 B (degrid), measured by ncu on the 0.05-scale workload and
+            # scaled by visibilities
+            "traffic": int((95.0 if dom == "grid" else 113.0) * nvis),
+            "alg_bytes_per_launch": int(dom_bytes / launches_per_call),
             "fp32": {"achieved_tflops": round(flops_pass / (ms_step * 1e-3) / 1e12, 2),
                      "peak_tflops_nominal": round(fp32_peak, 1),
                      "frac": round(flops_pass / (ms_step * 1e-3) / 1e12 / fp32_peak, 4)},

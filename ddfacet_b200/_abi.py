@@ -89,6 +89,10 @@ SIGNATURES = {
                             C.c_int, _vp]),
     "ddfg_degrid": (C.c_int, [C.POINTER(VisSet), C.POINTER(Jones), C.POINTER(Pol), C.POINTER(Facet), C.c_int,
                               _vp]),
+    "ddfg_degrid_adjoint": (C.c_int, [C.POINTER(VisSet), C.POINTER(Jones), C.POINTER(Pol), C.POINTER(Facet),
+                                      C.c_int, _vp]),
+    "ddfg_degrid_jones_grad": (C.c_int, [C.POINTER(VisSet), C.POINTER(Jones), C.POINTER(Pol), C.POINTER(Facet),
+                                         C.c_int, _vp, _vp]),
     "ddfg_sort_plan_workspace_size": (C.c_size_t, [_i64]),
     "ddfg_sort_plan_build": (C.c_int, [C.POINTER(VisSet), C.POINTER(Facet), C.POINTER(SortPlan), _vp, C.c_size_t,
                                        _vp]),

@@ -279,3 +279,35 @@ extern "C" int ddfg_degrid(const ddfg_vis *vs, const ddfg_jones *js, const ddfg_
   if (nfacets == 0 || vs->nblocks == 0) return DDFG_OK;
   return ddfg_launch_degrid(vs, js, facets, nfacets, policy, pol->npol, ddfg_num_ctas(4), (cudaStream_t)stream);
 }
+
+extern "C" int ddfg_degrid_adjoint(const ddfg_vis *vs, const ddfg_jones *js, const ddfg_pol *pol,
+                                   const ddfg_facet *facets, int nfacets, void *stream) {
+  g_err[0] = 0;
+  int policy = -1;
+  int rc = degrid_checks(vs, js, pol, facets, nfacets, &policy);
+  if (rc) return rc;
+  if (vs->nblocks > 0 && !vs->single_vis_blocks)
+    return ddfg_set_error(DDFG_EUNSUPPORTED, "degrid_adjoint: every block of the map must be one visibility");
+  if (nfacets == 0 || vs->nblocks == 0) return DDFG_OK;
+  return ddfg_launch_degrid_adjoint(vs, js, facets, nfacets, policy, pol->npol, ddfg_num_ctas(4),
+                                    (cudaStream_t)stream);
+}
+
+extern "C" int ddfg_degrid_jones_grad(const ddfg_vis *vs, const ddfg_jones *js, const ddfg_pol *pol,
+                                      const ddfg_facet *facets, int nfacets, void *grad_kms, void *stream) {
+  g_err[0] = 0;
+  int policy = -1;
+  int rc = degrid_checks(vs, js, pol, facets, nfacets, &policy);
+  if (rc) return rc;
+  if (vs->nblocks > 0 && !vs->single_vis_blocks)
+    return ddfg_set_error(DDFG_EUNSUPPORTED, "degrid_jones_grad: every block of the map must be one visibility");
+  if (js->mode == 0 || !js->kms || js->beam || js->interp_mode != 0 || !js->apply_amp || !js->apply_phase ||
+      js->scale_jones)
+    return ddfg_set_error(DDFG_EUNSUPPORTED,
+                          "degrid_jones_grad: needs kMS Jones only, nearest direction, no amplitude/phase "
+                          "normalisation");
+  if (!grad_kms) return ddfg_set_error(DDFG_EINVAL, "degrid_jones_grad: null gradient array");
+  if (nfacets == 0 || vs->nblocks == 0) return DDFG_OK;
+  return ddfg_launch_jones_grad(vs, js, facets, nfacets, policy, pol->npol, grad_kms, ddfg_num_ctas(4),
+                                (cudaStream_t)stream);
+}

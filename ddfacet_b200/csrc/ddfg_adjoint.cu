@@ -1,0 +1,252 @@
+// Backward passes of the degridder, for differentiating a visibility prediction.
+//
+// For single-visibility blocks the degridder's prediction of facet f at visibility v is linear
+// in the facet's model grid G_f:
+//     P_v = d ph_v J0 L(s) J1^H,   s_p = sum_t CF[t] G_f[p][cell_t],
+// with L the Stokes -> correlation map of the policy (Stokes.h:101-192), J0/J1 the antenna Jones
+// terms, ph_v = exp(+i nu angle) and d the smearing factor (degridder.h:202-261).  Given the
+// gradient g = dLoss/dP* of a real loss, the backward passes are:
+//   * model grids (the adjoint, exact in exact arithmetic): G_f[p][cell_t] += conj(CF[t]) *
+//     L^H(d conj(ph_v) J0^H g J1)_p -- a gridding pass with conjugated taps, the adjoint Stokes
+//     map (no 1/2 factors) and no weights;
+//   * Jones terms (J = J_kMS, nearest direction, no amplitude/phase normalisation): with
+//     Q = d ph L(s) J1^H and R = d ph J0 L(s), dLoss/dJ0* += g Q^H and dLoss/dJ1* += g^H R.
+// Phases, smearing and Jones terms are recomputed from the same inputs as the forward pass.
+#include <cuda_runtime.h>
+
+#include "ddfg_common.cuh"
+#include "ddfg_degridblock.cuh"
+#include "ddfg_gridblock.cuh"
+#include "ddfg_internal.h"
+#include "ddfg_taps.cuh"
+
+namespace ddfg {
+
+// g as a 2x2 correlation matrix, the way the degridder maps its 2x2 prediction onto the
+// visibility's correlations (4: all; 2: [0] and [3]; 1: [0]).
+__device__ __forceinline__ M2 load_corr_matrix(const ddfg_vis &vs, int64_t irow, int ch) {
+  const float2 *vp = (const float2 *)vs.vis + (irow * vs.nchan + ch) * (int64_t)vs.ncorr;
+  M2 g;
+  g.v[1] = czero();
+  g.v[2] = czero();
+  if (vs.ncorr == 4) {
+    const float4 a = *(const float4 *)vp, c = *(const float4 *)(vp + 2);
+    g.v[0] = make_float2(a.x, a.y); g.v[1] = make_float2(a.z, a.w);
+    g.v[2] = make_float2(c.x, c.y); g.v[3] = make_float2(c.z, c.w);
+  } else if (vs.ncorr == 2) {
+    g.v[0] = vp[0]; g.v[3] = vp[1];
+  } else {
+    g.v[0] = vp[0]; g.v[3] = czero();
+  }
+  return g;
+}
+
+// L^H: the adjoint of corr_from_stokes, column by column.
+template <int NPOL>
+__device__ __forceinline__ void stokes_adjoint(int pol, const M2 &g, float2 *s) {
+#pragma unroll
+  for (int p = 0; p < NPOL; ++p) {
+    float2 e[4] = {czero(), czero(), czero(), czero()};
+    e[p] = make_float2(1.f, 0.f);
+    const M2 col = corr_from_stokes(pol, e);
+    float2 acc = czero();
+#pragma unroll
+    for (int c = 0; c < 4; ++c) acc = cadd(acc, cmul(cconj(col.v[c]), g.v[c]));
+    s[p] = acc;
+  }
+}
+
+// The adjoint record of visibility `in` on facet f: footprint by the degridder's geometry and
+// value L^H(d conj(ph) J0^H g J1).
+template <int NPOL>
+__device__ __forceinline__ void adjoint_record(const DSingleIn &in, const ddfg_vis &vs, const ddfg_jones &js,
+                                               const ddfg_facet &f, int policy, double n0m1, GridRecord<NPOL> &rec) {
+  rec.valid = false;
+  if (!degrid_single_geom_in(in, f, rec.g)) return;
+  M2 gm = load_corr_matrix(vs, in.irow, in.ch);
+  if (js.mode != 0) {
+    M2 j0, j1;
+    float bb;
+    jones_pair_at(js, f.idir_kms, f.idir_beam, in.jx, in.U, in.V, j0, j1, bb);
+    gm = m2_times(m2_times(m2_herm(j0), gm), j1);
+  }
+  const float dec = (float)decorr_factor(vs, f, in.nu, in.irow);
+  const float2 ph = cscale(phasor_turns(in.nu * (in.U * f.l0 + in.V * f.m0 + in.W * n0m1) * kInvC), dec);
+  gm = m2_scale(gm, cconj(ph));
+  float2 s[4];
+  stokes_adjoint<NPOL>(policy, gm, s);
+#pragma unroll
+  for (int p = 0; p < NPOL; ++p) rec.stokes[p] = s[p];
+  rec.valid = true;
+  rec.gridchan = in.gridchan;
+}
+
+template <int NPOL, int SLOTS>
+__global__ void __launch_bounds__(256) degrid_adjoint_kernel(const ddfg_vis vs, const ddfg_jones js,
+                                                             const FacetPack pack, int policy) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  ddfg_facet *sf = (ddfg_facet *)smem_raw;
+  double *s_n0m1 = (double *)(sf + DDFG_FACETS_PER_LAUNCH);
+  stage_facets(pack, sf);
+  __syncthreads();
+  if (threadIdx.x < pack.n) {
+    const ddfg_facet &f = sf[threadIdx.x];
+    s_n0m1[threadIdx.x] = sqrt(1. - f.l0 * f.l0 - f.m0 * f.m0) - 1.;
+  }
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  const int warp = threadIdx.x >> 5;
+  const int nwarps = blockDim.x >> 5;
+  const int64_t nstripes = (vs.nblocks + 31) / 32;
+  LaneTaps<SLOTS> lt;
+  lt.reset();
+  for (int64_t s = (int64_t)blockIdx.x * nwarps + warp; s < nstripes; s += (int64_t)gridDim.x * nwarps) {
+    const int64_t b = s * 32 + lane;
+    DSingleIn in;
+    in.valid = false;
+    if (b < vs.nblocks) degrid_load_single(vs, js, b, in);
+    if (!__any_sync(0xffffffffu, in.valid)) continue;
+    for (int fi = 0; fi < pack.n; ++fi) {
+      const ddfg_facet &f = sf[fi];
+      GridRecord<NPOL> rec;
+      adjoint_record<NPOL>(in, vs, js, f, policy, s_n0m1[fi], rec);
+      scatter_records<NPOL, SLOTS, true>(rec, f, min(NPOL, f.npol), lt, lane);
+    }
+  }
+}
+
+// dLoss/dJ_kMS* for every visibility and facet: the forward gather of the model grid, then the
+// two antenna terms, reduced into the gradient array (same layout as the Jones array).
+template <int NPOL, int SLOTS>
+__global__ void __launch_bounds__(256) jones_grad_kernel(const ddfg_vis vs, const ddfg_jones js,
+                                                         const FacetPackD pack, int policy, float2 *grad) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  ddfg_facet *sf = (ddfg_facet *)smem_raw;
+  double *s_n0m1 = (double *)(sf + DDFG_FACETS_PER_LAUNCH);
+  float2 *partial = (float2 *)(s_n0m1 + DDFG_FACETS_PER_LAUNCH);
+  stage_facets(pack, sf);
+  __syncthreads();
+  if (threadIdx.x < pack.n) {
+    const ddfg_facet &f = sf[threadIdx.x];
+    s_n0m1[threadIdx.x] = sqrt(1. - f.l0 * f.l0 - f.m0 * f.m0) - 1.;
+  }
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  const int warp = threadIdx.x >> 5;
+  const int nwarps = blockDim.x >> 5;
+  const int64_t nstripes = (vs.nblocks + 31) / 32;
+  float2 *wpart = partial + warp * 32 * 32;
+  LaneTaps<SLOTS> lt;
+  lt.reset();
+  const size_t na = (size_t)js.kms_dims[2], nch = (size_t)js.kms_dims[3], nd = (size_t)js.kms_dims[1];
+  const float2 *J = (const float2 *)js.kms;
+  for (int64_t s = (int64_t)blockIdx.x * nwarps + warp; s < nstripes; s += (int64_t)gridDim.x * nwarps) {
+    const int64_t b = s * 32 + lane;
+    DSingleIn in;
+    in.valid = false;
+    if (b < vs.nblocks) degrid_load_single(vs, js, b, in);
+    if (!__any_sync(0xffffffffu, in.valid)) continue;
+    M2 g;
+    if (in.valid) g = load_corr_matrix(vs, in.irow, in.ch);
+    for (int fi = 0; fi < pack.n; ++fi) {
+      const ddfg_facet &f = sf[fi];
+      BlockGeom geo;
+      const bool valid = degrid_single_geom_in(in, f, geo);
+      TapJob job;
+      if (valid) job = tap_job(geo, in.gridchan, f);
+      float2 mine[NPOL];
+      gather_records<NPOL, SLOTS>(valid, job, f, lt, wpart, lane, mine);
+      if (valid) {
+      float2 sv[4];
+#pragma unroll
+      for (int p = 0; p < 4; ++p) sv[p] = (p < NPOL) ? mine[p] : czero();
+      const M2 m = corr_from_stokes(policy, sv);
+      const size_t o0 = (((size_t)in.jx.tk * nd + (size_t)f.idir_kms) * na + (size_t)in.jx.a0) * nch * 4 +
+                        (size_t)in.jx.ck * 4;
+      const size_t o1 = (((size_t)in.jx.tk * nd + (size_t)f.idir_kms) * na + (size_t)in.jx.a1) * nch * 4 +
+                        (size_t)in.jx.ck * 4;
+      M2 j0, j1;
+#pragma unroll
+      for (int p = 0; p < 4; ++p) {
+        j0.v[p] = J[o0 + p];
+        j1.v[p] = J[o1 + p];
+      }
+      const float dec = (float)decorr_factor(vs, f, in.nu, in.irow);
+      const float2 ph = cscale(phasor_turns(in.nu * (in.U * f.l0 + in.V * f.m0 + in.W * s_n0m1[fi]) * kInvC), dec);
+      const M2 q = m2_scale(m2_times(m, m2_herm(j1)), ph);  // d ph L(s) J1^H
+      const M2 r = m2_scale(m2_times(j0, m), ph);           // d ph J0 L(s)
+      const M2 d0 = m2_times(g, m2_herm(q));
+      const M2 d1 = m2_times(m2_herm(g), r);
+#pragma unroll
+      for (int p = 0; p < 4; ++p) {
+        red_add(grad + o0 + p, d0.v[p]);
+        red_add(grad + o1 + p, d1.v[p]);
+      }
+      }
+    }
+  }
+}
+
+}  // namespace ddfg
+
+using namespace ddfg;
+
+int ddfg_launch_degrid_adjoint(const ddfg_vis *vs, const ddfg_jones *js, const ddfg_facet *facets, int nfacets,
+                               int policy, int nvispol, int num_ctas, cudaStream_t stream) {
+  int max_support = 1;
+  for (int i = 0; i < nfacets; ++i) max_support = max(max_support, facets[i].max_support);
+  const int slots = tap_slots(max_support);
+  const size_t smem = sizeof(ddfg_facet) * DDFG_FACETS_PER_LAUNCH + sizeof(double) * DDFG_FACETS_PER_LAUNCH;
+  for (int f0 = 0; f0 < nfacets; f0 += DDFG_FACETS_PER_LAUNCH) {
+    FacetPack pack;
+    pack.n = min(DDFG_FACETS_PER_LAUNCH, nfacets - f0);
+    for (int i = 0; i < pack.n; ++i) pack.f[i] = facets[f0 + i];
+#define LAUNCH_A(NP, SL) degrid_adjoint_kernel<NP, SL><<<num_ctas, 256, smem, stream>>>(*vs, *js, pack, policy)
+#define LAUNCH_A_NP(SL)              \
+  switch (nvispol) {                 \
+    case 1: LAUNCH_A(1, SL); break;  \
+    case 2: LAUNCH_A(2, SL); break;  \
+    case 3: LAUNCH_A(3, SL); break;  \
+    default: LAUNCH_A(4, SL); break; \
+  }
+    if (slots == 2) { LAUNCH_A_NP(2) } else if (slots == 4) { LAUNCH_A_NP(4) } else { LAUNCH_A_NP(8) }
+#undef LAUNCH_A_NP
+#undef LAUNCH_A
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return ddfg_set_error(DDFG_ECUDA, "degrid_adjoint launch: %s", cudaGetErrorString(e));
+  }
+  return DDFG_OK;
+}
+
+int ddfg_launch_jones_grad(const ddfg_vis *vs, const ddfg_jones *js, const ddfg_facet *facets, int nfacets,
+                           int policy, int nvispol, void *grad, int num_ctas, cudaStream_t stream) {
+  int max_support = 1;
+  for (int i = 0; i < nfacets; ++i) max_support = max(max_support, facets[i].max_support);
+  const int slots = tap_slots(max_support);
+  const size_t smem = sizeof(ddfg_facet) * DDFG_FACETS_PER_LAUNCH + sizeof(double) * DDFG_FACETS_PER_LAUNCH +
+                      (nvispol == 1 ? 8 * kPartialBytesPerWarp : 0);
+  float2 *g = (float2 *)grad;
+  for (int f0 = 0; f0 < nfacets; f0 += DDFG_FACETS_PER_LAUNCH) {
+    FacetPackD pack;
+    pack.n = min(DDFG_FACETS_PER_LAUNCH, nfacets - f0);
+    for (int i = 0; i < pack.n; ++i) pack.f[i] = facets[f0 + i];
+#define LAUNCH_J(NP, SL)                                                                                      \
+  do {                                                                                                        \
+    cudaFuncSetAttribute(jones_grad_kernel<NP, SL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);  \
+    jones_grad_kernel<NP, SL><<<num_ctas, 256, smem, stream>>>(*vs, *js, pack, policy, g);                    \
+  } while (0)
+#define LAUNCH_J_NP(SL)              \
+  switch (nvispol) {                 \
+    case 1: LAUNCH_J(1, SL); break;  \
+    case 2: LAUNCH_J(2, SL); break;  \
+    case 3: LAUNCH_J(3, SL); break;  \
+    default: LAUNCH_J(4, SL); break; \
+  }
+    if (slots == 2) { LAUNCH_J_NP(2) } else if (slots == 4) { LAUNCH_J_NP(4) } else { LAUNCH_J_NP(8) }
+#undef LAUNCH_J_NP
+#undef LAUNCH_J
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return ddfg_set_error(DDFG_ECUDA, "jones_grad launch: %s", cudaGetErrorString(e));
+  }
+  return DDFG_OK;
+}

@@ -21,149 +21,9 @@
 #include "ddfg_common.cuh"
 #include "ddfg_gridblock.cuh"
 #include "ddfg_internal.h"
+#include "ddfg_taps.cuh"
 
 namespace ddfg {
-
-// Warp-cooperative tap scatter of the warp's 32 records onto facet f (gridder.h:353-362): each
-// record's footprint, CF offset and support travel in three shuffles; each lane keeps the cell
-// offsets of its taps for as long as the support and grid width stay the same.  Up to four
-// records of equal support are issued together so their CF loads are in flight at once.
-// Must be called by all 32 lanes.
-template <int NPOL, int SLOTS>
-__device__ __forceinline__ void scatter_records(const GridRecord<NPOL> &rec, const ddfg_facet &f, int npol_used,
-                                                LaneTaps<SLOTS> &lt, int lane) {
-  float2 *grid = (float2 *)f.grid;
-  const float2 *cfd = (const float2 *)f.cf_data;
-  const int plane_sz = f.nx * f.ny;
-  TapJob job;
-  if (rec.valid) job = tap_job(rec.g, rec.gridchan, f);
-  unsigned mask = __ballot_sync(0xffffffffu, rec.valid);
-  if (!mask) return;
-  // Fast path: every valid record of the stripe has the same support, which fits the slots (the
-  // usual case: a stripe is one row's channels, all on one W plane).  The lane's tap pointers
-  // are formed once, and each record costs three shuffles, its CF loads and the reductions.
-  const int first = __ffs(mask) - 1;
-  const int s_inv0 = __shfl_sync(0xffffffffu, rec.valid ? job.s_inv : 0, first);
-  const int S0 = s_inv0 & 255;
-  if (S0 * S0 <= 32 * SLOTS && __all_sync(0xffffffffu, !rec.valid || (job.s_inv & 255) == S0)) {
-    lt.set(s_inv0, f.nx, lane);
-    const float2 *cf_lane = cfd + lane;
-    float2 *g_lane[SLOTS];
-    bool on[SLOTS];
-#pragma unroll
-    for (int k = 0; k < SLOTS; ++k) {
-      on[k] = lt.off[k] >= 0;
-      g_lane[k] = grid + (on[k] ? lt.off[k] : 0);
-    }
-    while (mask) {
-      int src[4];
-      int nr = 0;
-#pragma unroll
-      for (int r = 0; r < 4; ++r) {
-        src[r] = mask ? __ffs(mask) - 1 : src[0];
-        if (mask) {
-          mask &= mask - 1;
-          ++nr;
-        }
-      }
-      int base[4], cfo[4];
-      float2 sv[4][NPOL];
-#pragma unroll
-      for (int r = 0; r < 4; ++r) {
-        base[r] = __shfl_sync(0xffffffffu, job.base, src[r]);
-        cfo[r] = __shfl_sync(0xffffffffu, job.cfoff, src[r]);
-#pragma unroll
-        for (int p = 0; p < NPOL; ++p) {
-          sv[r][p].x = __shfl_sync(0xffffffffu, rec.stokes[p].x, src[r]);
-          sv[r][p].y = __shfl_sync(0xffffffffu, rec.stokes[p].y, src[r]);
-        }
-      }
-      float2 c[4][SLOTS];
-#pragma unroll
-      for (int r = 0; r < 4; ++r)
-#pragma unroll
-        for (int k = 0; k < SLOTS; ++k) c[r][k] = on[k] ? __ldg(cf_lane + cfo[r] + 32 * k) : czero();
-#pragma unroll
-      for (int r = 0; r < 4; ++r) {
-        if (r < nr) {
-#pragma unroll
-          for (int k = 0; k < SLOTS; ++k) {
-            if (on[k]) {
-              float2 *cell = g_lane[k] + base[r];
-#pragma unroll
-              for (int p = 0; p < NPOL; ++p)
-                if (NPOL == 1 || p < npol_used) red_add(cell + (size_t)p * plane_sz, cmul(sv[r][p], c[r][k]));
-            }
-          }
-        }
-      }
-    }
-    return;
-  }
-  while (mask) {
-    int src[4];
-    int nr = 0;
-#pragma unroll
-    for (int r = 0; r < 4; ++r) {
-      src[r] = mask ? __ffs(mask) - 1 : -1;
-      if (mask) {
-        mask &= mask - 1;
-        ++nr;
-      }
-    }
-    TapJob j[4];
-    float2 sv[4][NPOL];
-#pragma unroll
-    for (int r = 0; r < 4; ++r) {
-      const int sr = src[r] >= 0 ? src[r] : src[0];
-      j[r] = shfl_job(job, sr);
-#pragma unroll
-      for (int p = 0; p < NPOL; ++p) {
-        sv[r][p].x = __shfl_sync(0xffffffffu, rec.stokes[p].x, sr);
-        sv[r][p].y = __shfl_sync(0xffffffffu, rec.stokes[p].y, sr);
-      }
-    }
-    const int S = j[0].s_inv & 255;
-    bool same = S * S <= 32 * SLOTS;
-#pragma unroll
-    for (int r = 1; r < 4; ++r) same = same && (r >= nr || (j[r].s_inv & 255) == S);
-    if (same) {
-      lt.set(j[0].s_inv, f.nx, lane);
-      float2 c[4][SLOTS];
-#pragma unroll
-      for (int r = 0; r < 4; ++r)
-#pragma unroll
-        for (int k = 0; k < SLOTS; ++k)
-          c[r][k] = (r < nr && lt.off[k] >= 0) ? __ldg(cfd + j[r].cfoff + lane + 32 * k) : czero();
-#pragma unroll
-      for (int r = 0; r < 4; ++r) {
-        if (r >= nr) break;
-#pragma unroll
-        for (int k = 0; k < SLOTS; ++k) {
-          if (lt.off[k] >= 0) {
-            float2 *cell = grid + (j[r].base + lt.off[k]);
-#pragma unroll
-            for (int p = 0; p < NPOL; ++p)
-              if (p < npol_used) red_add(cell + (size_t)p * plane_sz, cmul(sv[r][p], c[r][k]));
-          }
-        }
-      }
-    } else {
-      for (int r = 0; r < nr; ++r) {
-        const int Sr = j[r].s_inv & 255;
-        const unsigned inv = (unsigned)j[r].s_inv >> 8;
-        for (int t = lane; t < Sr * Sr; t += 32) {
-          const int sy = (int)(((unsigned)t * inv) >> 16);
-          const float2 cv = __ldg(cfd + j[r].cfoff + t);
-          float2 *cell = grid + (j[r].base + sy * f.nx + (t - sy * Sr));
-#pragma unroll
-          for (int p = 0; p < NPOL; ++p)
-            if (p < npol_used) red_add(cell + (size_t)p * plane_sz, cmul(sv[r][p], cv));
-        }
-      }
-    }
-  }
-}
 
 template <int NPOL, int SLOTS, bool SINGLE>
 __global__ void __launch_bounds__(256) grid_kernel(const ddfg_vis vs, const ddfg_jones js, const FacetPack pack,

@@ -19,3 +19,7 @@ int ddfg_launch_grid_sorted(const ddfg_vis *vs, const ddfg_jones *js, const ddfg
 int ddfg_launch_degrid_sorted(const ddfg_vis *vs, const ddfg_jones *js, const ddfg_facet *facets, int nfacets,
                               int policy, int nvispol, const ddfg_sort_plan *plan, int max_support,
                               int facets_per_launch, cudaStream_t stream);
+int ddfg_launch_degrid_adjoint(const ddfg_vis *vs, const ddfg_jones *js, const ddfg_facet *facets, int nfacets,
+                               int policy, int nvispol, int num_ctas, cudaStream_t stream);
+int ddfg_launch_jones_grad(const ddfg_vis *vs, const ddfg_jones *js, const ddfg_facet *facets, int nfacets,
+                           int policy, int nvispol, void *grad, int num_ctas, cudaStream_t stream);

@@ -164,6 +164,25 @@ int ddfg_grid(const ddfg_vis *vs, const ddfg_jones *js, const ddfg_pol *pol,
 int ddfg_degrid(const ddfg_vis *vs, const ddfg_jones *js, const ddfg_pol *pol,
                 const ddfg_facet *facets, int nfacets, void *stream);
 
+/* Backward pass of ddfg_degrid for the model grids.  ddfg_degrid subtracts a prediction P that
+ * is linear in the facets' model grids; given vs->vis = dLoss/dP* (the gradient of a real loss,
+ * complex64 [nrow][nchan][ncorr], read only), this adds P's adjoint applied to it to each
+ * facets[i].grid (+=): conj(CF) taps at the degridder's footprint, the adjoint Stokes map (for
+ * Stokes I from XX/YY: g_XX + g_YY), conj(phasor), J0^H g J1 and the smearing factor.  The
+ * facets carry the degridder's CF order (as for ddfg_degrid).  Maps whose every block is one
+ * visibility only (DDFG_EUNSUPPORTED otherwise).  No counterpart in the reference, whose
+ * degridder has no derivative. */
+int ddfg_degrid_adjoint(const ddfg_vis *vs, const ddfg_jones *js, const ddfg_pol *pol,
+                        const ddfg_facet *facets, int nfacets, void *stream);
+
+/* Backward pass of ddfg_degrid for the kMS Jones terms: with vs->vis = dLoss/dP* as above and
+ * facets[i].grid the model grids of the forward pass, adds dLoss/dJ* to grad_kms (complex64,
+ * the layout of js->kms, +=).  Needs kMS Jones only, nearest direction, no amplitude/phase
+ * normalisation, single-visibility blocks (DDFG_EUNSUPPORTED otherwise).  No counterpart in the
+ * reference. */
+int ddfg_degrid_jones_grad(const ddfg_vis *vs, const ddfg_jones *js, const ddfg_pol *pol,
+                           const ddfg_facet *facets, int nfacets, void *grad_kms, void *stream);
+
 /* Most blocks ddfg_bda_plan_noalloc accepts. */
 #define DDFG_BDA_PLAN_NOALLOC_MAX_BLOCKS (1 << 24)
 
