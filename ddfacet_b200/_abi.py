@@ -93,6 +93,10 @@ SIGNATURES = {
                                       C.c_int, _vp]),
     "ddfg_degrid_jones_grad": (C.c_int, [C.POINTER(VisSet), C.POINTER(Jones), C.POINTER(Pol), C.POINTER(Facet),
                                          C.c_int, _vp, _vp]),
+    "ddfg_weights_uv_index": (C.c_int, [_vp, _i64, _vp, _i32, _vp, _vp, _i32, _f64, _i64, _i64, _i64, _vp, _vp]),
+    "ddfg_weights_accumulate": (C.c_int, [_vp, _i64, _vp, _vp, _i64, _vp, _vp]),
+    "ddfg_weights_robust": (C.c_int, [_vp, _i64, _i32, _f64, _vp, _vp]),
+    "ddfg_weights_finalize": (C.c_int, [_vp, _vp, _i64, _vp, _i64, _vp]),
     "ddfg_sort_plan_workspace_size": (C.c_size_t, [_i64]),
     "ddfg_sort_plan_build": (C.c_int, [C.POINTER(VisSet), C.POINTER(Facet), C.POINTER(SortPlan), _vp, C.c_size_t,
                                        _vp]),

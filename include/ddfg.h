@@ -183,6 +183,37 @@ int ddfg_degrid_adjoint(const ddfg_vis *vs, const ddfg_jones *js, const ddfg_pol
 int ddfg_degrid_jones_grad(const ddfg_vis *vs, const ddfg_jones *js, const ddfg_pol *pol,
                            const ddfg_facet *facets, int nfacets, void *grad_kms, void *stream);
 
+/* ---- Imaging weights (uniform / Briggs uv-density grid) ------------------------------------
+ * The weight grid is float64 [nbands][npix] over the half uv-plane: npixx = 2 xymax + 1 cells in
+ * u (offset by xymax), xymax + 1 in v, npix = npixx (xymax + 1), cell = 1 / (SuperUniform FOV).
+ *
+ * ddfg_weights_uv_index replaces ClassVisServer._uv_to_index (DDFacet/Data/ClassVisServer.py:
+ * 981-1003): index[r][c] of every visibility (v < 0 flips (u, v); floor(u nu / c / cell) +
+ * xymax and floor(v nu / c / cell); + band_of_chan[c] * npix when nbands > 1; 0 where the weight
+ * is 0).  uvw [nrow][3] float64, freqs [nchan], weights float32 [nrow][nchan] with flagged
+ * visibilities already 0, index int32 [nrow][nchan] out.  Unlike the reference it does not flip
+ * the caller's uvw in place. */
+int ddfg_weights_uv_index(const double *uvw, int64_t nrow, const double *freqs, int32_t nchan,
+                          const float *weights, const int32_t *band_of_chan, int32_t nbands, double cell,
+                          int64_t xymax, int64_t npixx, int64_t npix, int32_t *index, void *stream);
+
+/* grid[index[i]] += weights[i] for every non-zero weight (pyAccumulateWeightsOntoGrid /
+ * ...NoSem, GridderSmearPols.cc:32-74).  Indices outside [0, grid_len) are skipped and set bit 0
+ * of *bad (a device word the caller clears and reads). */
+int ddfg_weights_accumulate(double *grid, int64_t grid_len, const float *weights, const int32_t *index,
+                            int64_t n, unsigned int *bad, void *stream);
+
+/* Briggs weighting (ClassVisServer.py:897-904): per band, grid = 1 + grid * s2 / avgW with
+ * s2 = numerator_sqrt^2 (numerator_sqrt = 5 * 10^-Robust) and avgW = sum grid^2 / sum grid.
+ * workspace: 2 * nbands doubles of device scratch. */
+int ddfg_weights_robust(double *grid, int64_t npix, int32_t nbands, double numerator_sqrt, double *workspace,
+                        void *stream);
+
+/* weights[i] /= grid[index[i]] (indices >= grid_len read cell 0), the uniform / Briggs
+ * normalisation of _finalizeWeights_handler (ClassVisServer.py:1036-1043). */
+int ddfg_weights_finalize(float *weights, const int32_t *index, int64_t n, const double *grid, int64_t grid_len,
+                          void *stream);
+
 /* Most blocks ddfg_bda_plan_noalloc accepts. */
 #define DDFG_BDA_PLAN_NOALLOC_MAX_BLOCKS (1 << 24)
 

@@ -14,6 +14,11 @@ The reference's Python modules are imported with stand-ins for the absent option
   grid_golden.npz  inputs and outputs of pyGridderWPol32 / pyDeGridderWPol on a small case
                    (4 correlations, Stokes I, per-visibility Jones, BDA blocks, flags)
   sw_golden.npz    ModFFTW.ConvolveGaussian of a facet mask (the spatial-weight smoothing)
+  weights_golden.npz  imaging weights: ClassVisServer._uv_to_index, the compiled
+                   pyAccumulateWeightsOntoGridNoSem, the Briggs step and
+                   ClassVisServer._finalizeWeights_handler on a small observation
+
+    python tests/golden/make_golden.py [/path/to/reference] [--only weights]
 """
 import os
 import sys
@@ -23,7 +28,9 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+_args = [a for a in sys.argv[1:] if not a.startswith("--") and a != "weights"]
+REF = _args[0] if _args else "/root/reference"
+ONLY = sys.argv[sys.argv.index("--only") + 1] if "--only" in sys.argv else None
 
 
 def _stub(name, **attrs):
@@ -81,7 +88,124 @@ class CFDict(dict):
         return self[name]
 
 
+def import_visserver():
+    """DDFacet.Data.ClassVisServer with inert stand-ins for the MS, beam and astronomy packages it
+    imports at module level (none of them is used by the weight functions), and the compiled
+    reference gridder module from oracle/_ref."""
+    class _Meta(type):
+        def __getattr__(cls, k):
+            if k.startswith("__"):
+                raise AttributeError(k)
+            return cls
+
+        def __call__(cls, *a, **k):
+            return cls
+
+    inert = _Meta("Inert", (), {})
+
+    class _Mod(types.ModuleType):
+        __path__ = []
+
+        def __getattr__(self, k):
+            if k.startswith("__"):
+                raise AttributeError(k)
+            return inert
+
+    def stub(name):
+        parts = name.split(".")
+        for i in range(1, len(parts) + 1):
+            n = ".".join(parts[:i])
+            if n not in sys.modules:
+                sys.modules[n] = _Mod(n)
+
+    for n in ("pyrap.tables", "pyrap.measures", "pyrap.quanta", "casacore.tables", "casacore.measures",
+              "casacore.quanta", "astropy.time", "astropy.io.fits", "astropy.wcs", "ephem"):
+        stub(n)
+    sys.path.insert(0, ROOT)
+    from oracle import ref
+    mod = ref.module()
+    sys.modules["DDFacet.cbuild.Gridder._pyGridderSmearPols3x"] = mod
+    sys.modules["DDFacet.cbuild.Gridder"].__dict__["_pyGridderSmearPols3x"] = mod
+    for _ in range(60):
+        try:
+            from DDFacet.Data import ClassVisServer
+            return ClassVisServer, mod
+        except ModuleNotFoundError as e:
+            for k in list(sys.modules):
+                if k.startswith("DDFacet.Data.Class") or k.startswith("DDFacet.Imager.Class"):
+                    del sys.modules[k]
+            stub(e.name)
+    raise RuntimeError("could not import ClassVisServer")
+
+
+class _MSW(dict):
+    def delete_item(self, k):
+        self.pop(k, None)
+
+
+def make_weights_golden():
+    import tempfile
+
+    V, mod = import_visserver()
+    sys.path.insert(0, ROOT)
+    from ddfacet_b200 import synth
+    obs = synth.make_observation(31, 8, 1500.0, 34.0, 40.0, 20 * 30.0 / 3600.0, 30.0, 8, 1.30e9, 1.45e9)
+    rng = np.random.default_rng(32)
+    nrow, nchan = obs.nrow, 8
+    freqs = obs.freqs
+    weights = rng.uniform(0.5, 2.0, (nrow, nchan)).astype(np.float32)
+    weights[rng.uniform(size=(nrow, nchan)) < 0.1] = 0          # flagged
+    rowflags = np.zeros(nrow, bool)
+    band_of_chan = np.array([0, 0, 0, 0, 1, 1, 1, 1], np.int32)
+    cell_rad, npix_image, super_uniform = 3.0 / 3600 * np.pi / 180, 512, 1.0
+    out = {"uvw": obs.uvw, "freqs": freqs, "weights_in": weights, "band_of_chan": band_of_chan,
+           "cell_rad": cell_rad, "npix_image": npix_image, "super_uniform": super_uniform}
+    uvmax = abs(obs.uvw[~rowflags, :2]).max() * freqs.max() / V._cc      # ClassVisServer.py:949
+    fov = cell_rad * npix_image                                          # ClassVisServer.py:868-883
+    cell = 1. / (super_uniform * fov)
+    xymax = int(np.floor(uvmax / cell)) + 1
+    npixx = xymax * 2 + 1
+    npix = npixx * (xymax + 1)
+    out.update(uvmax=uvmax, cell=cell, xymax=xymax, npixx=npixx, npix=npix)
+
+    class Self:
+        DicoMSChanMapping = {0: band_of_chan}
+        ListMS = [types.SimpleNamespace(MSName="synthetic")]
+
+    for nbands in (1, 2):
+        self = Self()
+        self.Weighting = "briggs"
+        self._uv_to_index = lambda *a, _s=self: V.ClassVisServer._uv_to_index(_s, *a)
+        uv = obs.uvw[:, :2].copy()
+        index = V.ClassVisServer._uv_to_index(self, 0, uv, weights, freqs, cell, npix, npixx, nbands, xymax)
+        grid = np.zeros((nbands, npix), np.float64)
+        mod.pyAccumulateWeightsOntoGridNoSem(grid, weights.ravel(), index.ravel())
+        out[f"index_{nbands}"] = index
+        out[f"grid_{nbands}"] = grid.copy()
+        robust = 0.5                                                    # ClassVisServer.py:897-904
+        numeratorSqrt = 5.0 * 10 ** (-robust)
+        for band in range(nbands):
+            grid1 = grid[band, :]
+            avgW = (grid1 ** 2).sum() / grid1.sum()
+            sSq = numeratorSqrt ** 2 / avgW
+            grid1[...] = 1 + grid1 * sSq
+        out[f"grid_briggs_{nbands}"] = grid.copy()
+        with tempfile.TemporaryDirectory() as td:
+            msw = _MSW(weight=weights.copy(), uv=uv, cachepath=os.path.join(td, "w.npy"))
+            V.ClassVisServer._finalizeWeights_handler(self, {"grid": grid}, msw, 0, 0, freqs, cell, npix, npixx,
+                                                      nbands, xymax)
+            assert msw.get("success"), msw.get("error")
+            out[f"weights_briggs_{nbands}"] = np.load(os.path.join(td, "w.npy"))
+    out["robust"] = 0.5
+    np.savez_compressed(os.path.join(HERE, "weights_golden.npz"), **out)
+    print("weights golden written")
+
+
 def main():
+    if ONLY == "weights":
+        import_reference()
+        make_weights_golden()
+        return
     ModCF, SM, ModFFTW = import_reference()
     sys.path.insert(0, ROOT)
     from ddfacet_b200 import synth
@@ -156,6 +280,7 @@ def main():
     sw = ModFFTW.ConvolveGaussian(shareddict={"in": mask, "out": mask.copy()}, field_in="in", field_out="out", ch=0,
                                   CellSizeRad=1, GaussPars_ch=(10, 10, 0))
     np.savez_compressed(os.path.join(HERE, "sw_golden.npz"), mask=mask[0, 0], sw=np.asarray(sw).reshape(97, 97))
+    make_weights_golden()
     print("golden fixtures written to", HERE)
 
 
