@@ -22,7 +22,7 @@ from typing import List, Optional
 import numpy as np
 import torch
 
-from . import bda, cf, device as D, geometry, synth
+from . import bda, cf, device as D, geometry, pipeline, synth
 
 C_LIGHT = 299792458.0
 
@@ -159,3 +159,22 @@ def multifacet_dde(device=None, scale=1.0, seed=1002, nfacets_side=9, nchan=64, 
     if keep_host:
         w.host["vis"] = vis.cpu().pin_memory()
     return w
+
+
+def row_chunks(w: Workload, nchunks: int) -> List[pipeline.Chunk]:
+    """The workload's rows in nchunks time ranges (whole dumps), each with its own block map
+    (chunk-relative rows) and Jones row maps, as views of the device buffers."""
+    obs = w.host["obs"]
+    nbl = obs.nrow // obs.ntimes
+    dev = w.vs.vis.device
+    edges = np.round(np.linspace(0, obs.ntimes, nchunks + 1)).astype(np.int64) * nbl
+    out = []
+    for r0, r1 in zip(edges[:-1], edges[1:]):
+        r0, r1 = int(r0), int(r1)
+        if r1 <= r0:
+            continue
+        bmap = _plain_map_gpu(obs.A0[r0:r1], obs.A1[r0:r1], w.nchan, dev)
+        vs = D.VisData.create(w.vs.vis[r0:r1], w.vs.uvw[r0:r1], w.vs.flags[r0:r1], w.vs.weights[r0:r1], obs.freqs,
+                              w.host["chan_map"], bmap, device=dev)
+        out.append(pipeline.Chunk((r0, r1), vs, pipeline.jones_rows(w.jones, r0, r1)))
+    return out

@@ -2,7 +2,7 @@
 
 The oracle accumulates in complex128 with double products; the GPU path is FP32 with FP64
 phase/index arithmetic.  Bounds:
-  * gridding: <= 1e-5 relative RMS of the grid (the north-star figure) and weight sums to 1e-9;
+  * gridding: <= 1e-5 relative RMS of the grid and weight sums to 1e-9;
   * degridding: within 2x of the reference's own complex64 error against the same oracle (the
     prediction sums S*S products whose terms cancel, which the reference's float products
     already bound) and <= 1e-4.
