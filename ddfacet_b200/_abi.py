@@ -97,6 +97,9 @@ SIGNATURES = {
     "ddfg_weights_accumulate": (C.c_int, [_vp, _i64, _vp, _vp, _i64, _vp, _vp]),
     "ddfg_weights_robust": (C.c_int, [_vp, _i64, _i32, _f64, _vp, _vp]),
     "ddfg_weights_finalize": (C.c_int, [_vp, _vp, _i64, _vp, _i64, _vp]),
+    "ddfg_bda_mode1_count": (C.c_int, [_vp, _vp, _vp, _i32, _i32, _vp, _f64, _f64, _f64, _f64, _vp, _vp, _vp]),
+    "ddfg_bda_mode1_write": (C.c_int, [_vp, _vp, _vp, _i32, _i32, _vp, _f64, _f64, _f64, _f64, _vp, _vp, _vp, _vp,
+                                       _vp]),
     "ddfg_sort_plan_workspace_size": (C.c_size_t, [_i64]),
     "ddfg_sort_plan_build": (C.c_int, [C.POINTER(VisSet), C.POINTER(Facet), C.POINTER(SortPlan), _vp, C.c_size_t,
                                        _vp]),

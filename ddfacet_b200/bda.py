@@ -212,3 +212,54 @@ def plain_map(A0, A1, nchan, uvw=None):
     body[:, 1] = ch + 1
     body[:, 2] = np.repeat(rows.astype(np.int32), nchan)
     return m
+
+
+def smear_mapping_gpu(A0, A1, uvw, freqs, dfreq, dPhi, l, chan_map, device=None):
+    """Mode-1 map (``GiveBlocksRowsListBL_old`` for every baseline, packed as
+    ``collectSmearMapping`` does) built on the GPU by ddfg_bda_mode1_count / _write: the same
+    words as ``smear_mapping(..., mode=1)``.  Returns an int32 device tensor."""
+    import torch
+
+    from . import _abi, device as D
+
+    dev = D._dev(device)
+    A0 = np.asarray(A0)
+    A1 = np.asarray(A1)
+    freqs = np.asarray(freqs, np.float64)
+    nchan = freqs.size
+    # baselines in the order of their "a0:a1" key strings (autocorrelations excluded)
+    na = int(max(A0.max(), A1.max())) + 1 if A0.size else 1
+    pairs = np.unique(A0.astype(np.int64) * na + A1.astype(np.int64))
+    pairs = pairs[(pairs // na) != (pairs % na)]
+    order = sorted(range(pairs.size), key=lambda i: "%d:%d" % (pairs[i] // na, pairs[i] % na))
+    rank = np.full(na * na, -1, np.int64)
+    rank[pairs[order]] = np.arange(pairs.size)
+    a0 = torch.from_numpy(A0.astype(np.int64)).to(dev)
+    a1 = torch.from_numpy(A1.astype(np.int64)).to(dev)
+    key = torch.from_numpy(rank).to(dev)[a0 * na + a1]
+    srt, perm = torch.sort(key, stable=True)
+    keep = srt >= 0
+    rows = perm[keep].to(torch.int32).contiguous()
+    nbl = int(pairs.size)
+    counts = torch.bincount(srt[keep], minlength=nbl)
+    bl_off = torch.zeros(nbl + 1, dtype=torch.int64, device=dev)
+    bl_off[1:] = torch.cumsum(counts, 0)
+    uvw_d = D.to_device(uvw, torch.float64, dev)
+    cmap = D.to_device(np.asarray(chan_map, np.int32), torch.int32, dev)
+    nblk = torch.zeros(max(nbl, 1), dtype=torch.int64, device=dev)
+    nwords = torch.zeros(max(nbl, 1), dtype=torch.int64, device=dev)
+    lib = _abi.lib()
+    st = D._stream_ptr()
+    nu0 = float(np.max(freqs))
+    args = (uvw_d.data_ptr(), rows.data_ptr(), bl_off.data_ptr(), nbl, nchan, cmap.data_ptr(), float(dfreq),
+            float(dPhi), float(l), nu0)
+    _abi.check(lib.ddfg_bda_mode1_count(*args, nblk.data_ptr(), nwords.data_ptr(), st))
+    blk_off = torch.cumsum(nblk, 0) - nblk
+    word_off = torch.cumsum(nwords, 0) - nwords
+    nb = int(nblk[:nbl].sum().item())
+    nw = int(nwords[:nbl].sum().item())
+    m = torch.empty(2 + nb + nw, dtype=torch.int32, device=dev)
+    m[0:2] = torch.from_numpy(_header(nb)).to(dev)
+    _abi.check(lib.ddfg_bda_mode1_write(*args, blk_off.data_ptr(), word_off.data_ptr(), m[2:].data_ptr(),
+                                        m[2 + nb:].data_ptr(), st))
+    return m

@@ -214,6 +214,24 @@ int ddfg_weights_robust(double *grid, int64_t npix, int32_t nbands, double numer
 int ddfg_weights_finalize(float *weights, const int32_t *index, int64_t n, const double *grid, int64_t grid_len,
                           void *stream);
 
+/* ---- BDA block maps on the GPU (mode 1) -----------------------------------------------------
+ * Replace GiveBlocksRowsListBL_old (DDFacet/Data/ClassSmearMapping.py:496-625), run per baseline
+ * by the reference's process pool, and collectSmearMapping's packing (:83-135): the map's words
+ * are identical.  rows: the visibility rows grouped by baseline in "a0:a1" key-string order,
+ * ascending within a baseline (autocorrelations left out); bl_off [nbl + 1] the group bounds;
+ * uvw [nrow][3]; chan_map [nchan] channel -> grid band; dfreq the channel width; dphi =
+ * sqrt(6 (1 - Decorr)); l the field radius; nu0 = max frequency.
+ * ddfg_bda_mode1_count writes each baseline's block and word counts ([nbl] int64 each);
+ * ddfg_bda_mode1_write writes the block sizes (sizes, from the map's word 2) and blocks (body,
+ * after the sizes) at the exclusive scans blk_off / word_off of those counts. */
+int ddfg_bda_mode1_count(const double *uvw, const int32_t *rows, const int64_t *bl_off, int32_t nbl,
+                         int32_t nchan, const int32_t *chan_map, double dfreq, double dphi, double l, double nu0,
+                         int64_t *nblk, int64_t *nwords, void *stream);
+int ddfg_bda_mode1_write(const double *uvw, const int32_t *rows, const int64_t *bl_off, int32_t nbl,
+                         int32_t nchan, const int32_t *chan_map, double dfreq, double dphi, double l, double nu0,
+                         const int64_t *blk_off, const int64_t *word_off, int32_t *sizes, int32_t *body,
+                         void *stream);
+
 /* Most blocks ddfg_bda_plan_noalloc accepts. */
 #define DDFG_BDA_PLAN_NOALLOC_MAX_BLOCKS (1 << 24)
 
