@@ -269,6 +269,19 @@ def run_gpu(args):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms_total = float(t.item())
     ms_step = ms_total / args.steps
+
+    # The same step captured once in a CUDA graph and replayed (device.capture_graph).
+    graph = D.capture_graph(step)
+    torch.cuda.synchronize()
+    gr0 = torch.cuda.Event(enable_timing=True)
+    gr1 = torch.cuda.Event(enable_timing=True)
+    gr0.record(stream)
+    for _ in range(max(1, min(args.steps, 3))):
+        graph.replay()
+    gr1.record(stream)
+    torch.cuda.synchronize()
+    graph_ms = gr0.elapsed_time(gr1) / max(1, min(args.steps, 3))
+    del graph
     degrid_ms = float(np.mean([e[0].elapsed_time(e[1]) for e in evs]))
     grid_ms = float(np.mean([e[1].elapsed_time(e[2]) for e in evs]))
 
@@ -411,7 +424,8 @@ def run_gpu(args):
             "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
             "scale": args.scale,
         },
-        "kernels_ms": {"degrid_call": round(degrid_ms, 3), "grid_call": round(grid_ms, 3)},
+        "kernels_ms": {"degrid_call": round(degrid_ms, 3), "grid_call": round(grid_ms, 3),
+                       "graph_replay_step": round(graph_ms, 3)},
         "plain": (None if plain_ms is None else
                   {"ms_per_step": round(plain_ms, 1), "value": round(world * nvis / (plain_ms * 1e-3) / 1e6, 3),
                    "what": "the same kernels, one facet per call (one launch per facet and direction)",

@@ -361,3 +361,21 @@ def degrid_sorted(vs: VisData, facets: List[FacetGrid], pol: _abi.Pol, plan: Sor
     vss = vs.struct()
     _abi.check(lib.ddfg_degrid_sorted(C.byref(vss), C.byref(js), C.byref(pol), arr, len(facets), C.byref(plan.st),
                                       int(facets_per_launch), _stream_ptr(stream)))
+
+
+def capture_graph(fn, warmup: int = 1):
+    """Record ``fn()`` -- a sequence of library calls on the current stream, such as a
+    degrid-then-grid step -- into a CUDA graph and return it (``g.replay()`` reruns it).  The
+    library's grid / degrid / FFT calls allocate nothing and never synchronise, so they capture
+    as they are; ``fn`` is run ``warmup`` times first on a side stream (this sets the kernels'
+    shared-memory attributes and loads the kernels before capture)."""
+    side = torch.cuda.Stream()
+    side.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(side):
+        for _ in range(warmup):
+            fn()
+    torch.cuda.current_stream().wait_stream(side)
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g):
+        fn()
+    return g
