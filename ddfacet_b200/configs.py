@@ -99,7 +99,9 @@ def _wterms(args):
 
 
 def build_wterms(tess_facets, cell, sup, nw, wmax, npix, freqs, overs, threads=8):
-    args = [(cell, sup, nw, wmax, npix, freqs, overs, (f.l0, f.m0), f.index) for f in tess_facets]
+    """W-term tables of every facet; npix is one padded grid side for all or one per facet."""
+    sides = list(npix) if np.ndim(npix) else [npix] * len(tess_facets)
+    args = [(cell, sup, nw, wmax, n, freqs, overs, (f.l0, f.m0), f.index) for f, n in zip(tess_facets, sides)]
     with cfut.ThreadPoolExecutor(threads) as ex:
         return list(ex.map(_wterms, args))
 

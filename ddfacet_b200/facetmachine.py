@@ -108,13 +108,15 @@ class FacetState:
 
 
 class FacetMachine:
-    """All facets of a regular ``nfacets_side`` x ``nfacets_side`` tessellation on one GPU."""
+    """All facets of a tessellation on one GPU: a regular ``nfacets_side`` x ``nfacets_side`` one
+    (ClassFacetMachine), or any ``tessellation`` such as ``geometry.voronoi_facets``
+    (ClassFacetMachineTessel), whose facets may differ in size."""
 
     def __init__(self, npix, cell_arcsec, nfacets_side, freqs, padding=1.7, nband=1, stokes_ids=(1,),
                  corr_ids=(9, 10, 11, 12), overs=11, support=7, nw=32, wmax=None, mixing_width=10.0, device=None,
-                 threads=8):
+                 threads=8, tessellation=None):
         self.device = D._dev(device)
-        self.tess = geometry.regular_facets(npix, nfacets_side, cell_arcsec, padding)
+        self.tess = tessellation or geometry.regular_facets(npix, nfacets_side, cell_arcsec, padding)
         self.cell = cell_arcsec
         self.freqs = np.asarray(freqs, np.float64)
         self.nband = nband
@@ -127,27 +129,32 @@ class FacetMachine:
         self.wmax = float(wmax)
         self.pol = D.make_pol(corr_ids, stokes_ids)
         t = self.tess
-        N = t.npix_padded
         self.npix_out = t.npix
         from .configs import build_wterms
 
-        wts = build_wterms(t.facets, cell_arcsec, support, nw, self.wmax, N, self.freqs, overs, threads=threads)
+        wts = build_wterms(t.facets, cell_arcsec, support, nw, self.wmax, [g.npix_padded for g in t.facets],
+                           self.freqs, overs, threads=threads)
         incr = (-cell_arcsec / 3600 * np.pi / 180, cell_arcsec / 3600 * np.pi / 180)
         radius_tot = t.cell_rad * t.npix * 0.5
         corners = [[-radius_tot, -radius_tot], [radius_tot, -radius_tot], [radius_tot, radius_tot],
                    [-radius_tot, radius_tot]]
-        rf = t.npix_facet * t.cell_rad * 0.5
-        rfp = N * t.cell_rad * 0.5
         self.facets: List[FacetState] = []
         norm = np.zeros((t.npix, t.npix), np.float32)
         dev = self.device
         for g, wt in zip(t.facets, wts):
-            poly = ([[g.l0 + rf, g.m0 - rf], [g.l0 - rf, g.m0 - rf], [g.l0 - rf, g.m0 + rf], [g.l0 + rf, g.m0 + rf]]
-                    if len(t.facets) > 1 else corners)
+            N = g.npix_padded
+            rf = g.npix_facet * t.cell_rad * 0.5
+            rfp = N * t.cell_rad * 0.5
+            if g.polygon is not None:
+                poly = g.polygon
+            elif len(t.facets) > 1:
+                poly = [[g.l0 + rf, g.m0 - rf], [g.l0 - rf, g.m0 - rf], [g.l0 - rf, g.m0 + rf], [g.l0 + rf, g.m0 + rf]]
+            else:
+                poly = corners
             sw = spatial_weight(poly, (g.l0 - rfp, g.l0 + rfp, g.m0 - rfp, g.m0 + rfp), N, corners, mixing_width)
             self._add_norm(norm, sw, g, N)
             tabs = D.CFTables.create(wt.Wplanes, wt.WplanesConj, overs, wt.RefWave, wt.wmax, device=dev)
-            common = dict(cf=tabs, incr=incr, cu=wt.Cu, cv=wt.Cv, l0=g.l0, m0=g.m0, idir_kms=g.index, idir_beam=0)
+            common = dict(cf=tabs, incr=incr, cu=wt.Cu, cv=wt.Cv, l0=g.l0, m0=g.m0, idir_kms=g.isol, idir_beam=0)
             z = lambda *s: torch.zeros(s, dtype=torch.float64, device=dev)  # noqa: E731
             fg = D.FacetGrid(grid=torch.zeros((nband, self.npol, N, N), dtype=torch.complex64, device=dev),
                              sumwt=z(nband, self.npol), sumjones=z(2, nband), sumjones_chan=z(2, self.freqs.size),

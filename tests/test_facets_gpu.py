@@ -10,18 +10,27 @@ import cases
 pytestmark = pytest.mark.gpu
 
 
-def _fm(nfs=3, npix=1200):
+def _fm(kind, nfs=3, npix=1200):
+    from ddfacet_b200 import geometry
     from ddfacet_b200.facetmachine import FacetMachine
 
     freqs = np.linspace(1.3e9, 1.45e9, 8)
+    tess = None
+    if kind == "voronoi":  # five directions: uneven facets (ClassFacetMachineTessel)
+        r = npix * 6.0 / 3600 * np.pi / 180 / 2
+        rng = np.random.default_rng(4)
+        tess = geometry.voronoi_facets(npix, 6.0, rng.uniform(-0.8 * r, 0.8 * r, 5), rng.uniform(-0.8 * r, 0.8 * r, 5),
+                                       1.7)
+        assert len({f.npix_padded for f in tess.facets}) > 1
     return FacetMachine(npix, 6.0, nfs, freqs, padding=1.7, nband=1, stokes_ids=(1,), corr_ids=(9, 10, 11, 12),
-                        support=7, nw=3, wmax=2000.0, mixing_width=10.0)
+                        support=7, nw=3, wmax=2000.0, mixing_width=10.0, tessellation=tess)
 
 
-def test_grid_to_image_and_stitch():
+@pytest.mark.parametrize("kind", ["regular", "voronoi"])
+def test_grid_to_image_and_stitch(kind):
     from oracle import facets as OF
 
-    fm = _fm()
+    fm = _fm(kind)
     rng = np.random.default_rng(0)
     grids = []
     for f in fm.facets:
@@ -41,10 +50,11 @@ def test_grid_to_image_and_stitch():
     assert cases.rel_rms(image, want) < 1e-5
 
 
-def test_image_to_grid():
+@pytest.mark.parametrize("kind", ["regular", "voronoi"])
+def test_image_to_grid(kind):
     from oracle import facets as OF
 
-    fm = _fm()
+    fm = _fm(kind)
     rng = np.random.default_rng(1)
     img = np.zeros((1, 1, fm.npix_out, fm.npix_out), np.float32)
     for _ in range(30):
