@@ -467,6 +467,48 @@ def nvis_w(w):
     return w.nrow * w.nchan
 
 
+def run_uneven(args):
+    """Uneven Voronoi facets with averaged BDA blocks (an additional workload, not the metric's
+    configuration): one degrid + grid step over all facets, device-resident, CUDA-event timed."""
+    import torch
+
+    from ddfacet_b200 import configs, device as D
+
+    dev = torch.device("cuda", 0)
+    t0 = time.perf_counter()
+    w = configs.uneven_bda(device=dev, scale=args.scale)
+    torch.cuda.synchronize()
+    setup_s = time.perf_counter() - t0
+    stream = torch.cuda.current_stream()
+
+    def step():
+        for f in w.facets_grid:
+            f.grid.zero_()
+        D.degrid(w.vs, w.facets_model, w.pol, w.jones)
+        D.grid(w.vs, w.facets_grid, w.pol, w.jones)
+
+    for _ in range(max(1, args.warmup)):
+        step()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    info = dict(w.info)
+    g = info.pop("grids")
+    print(json.dumps({"metric": METRIC, "value": round(w.nvis / (ms * 1e-3) / 1e6, 3), "unit": UNIT,
+                      "ms_per_step": round(ms, 1), "steps": args.steps, "warmup": max(1, args.warmup),
+                      "config": {"workload": f"uneven BDA: {w.nfacets} Voronoi facets (grids {min(g)}..{max(g)}), "
+                                             f"{w.nrow} rows x {w.nchan} ch x 4 corr ({w.nvis/1e6:.1f} Mvis), "
+                                             f"{info['nblocks']} BDA blocks, per-vis Jones", **info,
+                                 "scale": args.scale},
+                      "setup_s": round(setup_s, 1)}), flush=True)
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -503,10 +545,14 @@ def main():
     ap.add_argument("--scale", type=float, default=1.0)
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
     ap.add_argument("--plain", action="store_true", help="also time the one-facet-per-launch direct path")
+    ap.add_argument("--workload", default="multifacet_dde", choices=["multifacet_dde", "uneven_bda"],
+                    help="uneven_bda: an additional workload (Voronoi facets, averaged blocks)")
 
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload == "uneven_bda":
+        run_uneven(args)
     else:
         run_gpu(args)
 

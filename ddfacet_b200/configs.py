@@ -180,3 +180,62 @@ def row_chunks(w: Workload, nchunks: int) -> List[pipeline.Chunk]:
                               w.host["chan_map"], bmap, device=dev)
         out.append(pipeline.Chunk((r0, r1), vs, pipeline.jones_rows(w.jones, r0, r1)))
     return out
+
+
+def uneven_bda(device=None, scale=1.0, seed=1003, nfacets=25, npix_image=6000, cell=1.0, nchan=128, nw=32,
+               grid_decorr=0.02, nsrc=200):
+    """Uneven facets with baseline-dependent averaging: a 6000^2 image at 1"/pixel in a Voronoi
+    tessellation around 25 directions, 48 antennas in a 12 km log-radial layout, 6 h at 4 s,
+    128 channels 0.9-1.7 GHz, 4 correlations, per-facet per-antenna 5-min Jones; block map of
+    DDFacet's default mode 1 with GridDecorr 0.02 over the largest facet's field, built on the
+    GPU (every block averages a few rows and channels, more on short baselines)."""
+    dev = D._dev(device)
+    hours = 6.0 * scale
+    obs = synth.make_observation(seed, 48, 12000.0, 34.0, 40.0, hours, 4.0, nchan, 0.90e9, 1.70e9, layout="lograd")
+    rng = np.random.default_rng(seed + 5)
+    r = npix_image * cell / 3600 * np.pi / 180 / 2
+    tess = geometry.voronoi_facets(npix_image, cell, rng.uniform(-r, r, nfacets), rng.uniform(-r, r, nfacets), 1.7)
+    wmax = float(np.max(np.abs(obs.uvw[:, 2]))) * 1.001
+    wts = build_wterms(tess.facets, cell, 7, nw, wmax, [f.npix_padded for f in tess.facets], obs.freqs, 11)
+    l, m, s = synth.point_sky(seed + 1, nsrc, r * 0.95, flux=("powerlaw", 1e-4, 1.0))
+    uvw_d = torch.from_numpy(obs.uvw).to(dev)
+    freqs_d = torch.from_numpy(obs.freqs).to(dev)
+    ncorr = 4
+    vis = _gen_vis_gpu(uvw_d, freqs_d, l, m, s, ncorr, 1e-3, seed + 2, dev)
+    nrow = obs.nrow
+    flags = torch.zeros((nrow, nchan, ncorr), dtype=torch.uint8, device=dev)
+    weights = torch.ones((nrow, nchan), dtype=torch.float32, device=dev)
+    chan_map = np.zeros(nchan, np.int32)
+    lmax = max(f.npix_facet for f in tess.facets) * tess.cell_rad * np.sqrt(2) / 2
+    dfreq = float(obs.freqs[1] - obs.freqs[0])
+    bmap = bda.smear_mapping_gpu(obs.A0, obs.A1, uvw_d, obs.freqs, dfreq, np.sqrt(6 * grid_decorr), lmax, chan_map,
+                                 device=dev)
+    vs = D.VisData.create(vis, uvw_d, flags, weights, obs.freqs, chan_map, bmap, device=dev)
+    nt = int(np.ceil(hours * 3600 / 300.0))
+    J = synth.random_jones(seed + 3, nt, nfacets, 48, 1, 0.1)
+    tmap = np.minimum(((obs.times - obs.times.min()) // 300.0).astype(np.int32), nt - 1)
+    jd = D.JonesData(mode=1, kms=torch.from_numpy(J).to(dev), kms_tmap=torch.from_numpy(tmap).to(dev),
+                     kms_cmap=torch.zeros(nchan, dtype=torch.int32, device=dev),
+                     a0=torch.from_numpy(obs.A0).to(dev), a1=torch.from_numpy(obs.A1).to(dev),
+                     wavelength_mean=float(np.mean(C_LIGHT / obs.freqs)))
+    fg, fm = [], []
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(seed + 4)
+    incr = (-cell / 3600 * np.pi / 180, cell / 3600 * np.pi / 180)
+    for f, wt in zip(tess.facets, wts):
+        n = f.npix_padded
+        tabs = D.CFTables.create(wt.Wplanes, wt.WplanesConj, 11, wt.RefWave, wt.wmax, device=dev)
+        mg = torch.view_as_complex(torch.randn((1, 1, n, n, 2), generator=gen, device=dev).contiguous()) * 1e-3
+        common = dict(cf=tabs, incr=incr, cu=wt.Cu, cv=wt.Cv, l0=f.l0, m0=f.m0, idir_kms=f.isol, idir_beam=0)
+        fg.append(D.FacetGrid(grid=torch.zeros((1, 1, n, n), dtype=torch.complex64, device=dev),
+                              sumwt=torch.zeros((1, 1), dtype=torch.float64, device=dev),
+                              sumjones=torch.zeros((2, 1), dtype=torch.float64, device=dev),
+                              sumjones_chan=torch.zeros((2, nchan), dtype=torch.float64, device=dev), **common))
+        fm.append(D.FacetGrid(grid=mg, **common))
+    pol = D.make_pol([9, 10, 11, 12], [1])
+    w = Workload("uneven_bda", vs, fg, fm, jd, pol, nvis=nrow * nchan, nrow=nrow, nchan=nchan, ncorr=ncorr,
+                 nfacets=len(fg))
+    w.info = dict(npix=tess.npix, grids=[f.npix_padded for f in tess.facets], nw=nw, nblocks=vs.nblocks,
+                  vis_per_block=nrow * nchan / max(vs.nblocks, 1), wmax=wmax, nant=48, ntimes=obs.ntimes)
+    w.host = {"obs": obs, "wterms": wts, "tess": tess, "chan_map": chan_map}
+    return w

@@ -81,6 +81,63 @@ __global__ void __launch_bounds__(256) grid_kernel(const ddfg_vis vs, const ddfg
   }
 }
 
+// Averaged BDA blocks, facet-inner: each warp walks its 32 blocks for every facet of the launch
+// in turn (grid_block_record resets its Jones cache per block, so the order is free), so a
+// block's rows, visibilities, flags and weights are read from DRAM once per launch and from L1
+// for the other facets; per-facet shared accumulators hold the weight and Jones sums.
+template <int NPOL, int SLOTS>
+__global__ void __launch_bounds__(256) grid_block_fi_kernel(const ddfg_vis vs, const ddfg_jones js,
+                                                            const FacetPack pack, const GridParams gp,
+                                                            int acc_stride) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  ddfg_facet *sf = (ddfg_facet *)smem_raw;
+  double *s_n0m1 = (double *)(sf + DDFG_FACETS_PER_LAUNCH);
+  double *s_acc = s_n0m1 + DDFG_FACETS_PER_LAUNCH;
+  stage_facets(pack, sf);
+  for (int i = threadIdx.x; i < pack.n * acc_stride; i += blockDim.x) s_acc[i] = 0.;
+  __syncthreads();
+  if (threadIdx.x < pack.n) {
+    const ddfg_facet &f = sf[threadIdx.x];
+    s_n0m1[threadIdx.x] = sqrt(1. - f.l0 * f.l0 - f.m0 * f.m0) - 1.;
+  }
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  const int warp = threadIdx.x >> 5;
+  const int nwarps = blockDim.x >> 5;
+  const int64_t nstripes = (vs.nblocks + 31) / 32;
+  JonesCache jc;
+  LaneTaps<SLOTS> lt;
+  lt.reset();
+  for (int64_t s = (int64_t)blockIdx.x * nwarps + warp; s < nstripes; s += (int64_t)gridDim.x * nwarps) {
+    const int64_t b = s * 32 + lane;
+    for (int fi = 0; fi < pack.n; ++fi) {
+      const ddfg_facet &f = sf[fi];
+      const int npol_used = min(gp.nvispol, f.npol);
+      double *a = s_acc + (size_t)fi * acc_stride;
+      GridRecord<NPOL> rec;
+      rec.valid = false;
+      if (b < vs.nblocks) grid_block_record<NPOL>(vs, js, f, gp, b, s_n0m1[fi], rec, jc);
+      warp_add_block_sums<NPOL, false>(vs, js, f, gp, b, rec, npol_used, a, a + f.nband * f.npol,
+                                       a + f.nband * f.npol + 2 * f.nband, jc);
+      scatter_records<NPOL, SLOTS>(rec, f, npol_used, lt, lane);
+    }
+  }
+  __syncthreads();
+  for (int fi = 0; fi < pack.n; ++fi) {
+    const ddfg_facet &f = sf[fi];
+    const double *a = s_acc + (size_t)fi * acc_stride;
+    const int nsw = f.nband * f.npol;
+    for (int i = threadIdx.x; i < nsw; i += blockDim.x)
+      if (f.sumwt && a[i] != 0.) atomicAdd(&f.sumwt[i], a[i]);
+    if (js.mode != 0) {
+      for (int i = threadIdx.x; i < 2 * f.nband; i += blockDim.x)
+        if (f.sumjones && a[nsw + i] != 0.) atomicAdd(&f.sumjones[i], a[nsw + i]);
+      for (int i = threadIdx.x; i < 2 * vs.nchan; i += blockDim.x)
+        if (f.sumjones_chan && a[nsw + 2 * f.nband + i] != 0.) atomicAdd(&f.sumjones_chan[i], a[nsw + 2 * f.nband + i]);
+    }
+  }
+}
+
 // Single-visibility blocks, facet-inner: each warp loads its 32 visibilities' facet-independent
 // inputs (map entries, uvw, flags, weights, visibilities, Jones indices) once and grids them onto
 // every facet of the launch in turn, instead of re-reading them once per facet.  Per-facet weight
@@ -168,12 +225,34 @@ int ddfg_launch_grid(const ddfg_vis *vs, const ddfg_jones *js, const ddfg_facet 
   const size_t smem_fi = sizeof(ddfg_facet) * DDFG_FACETS_PER_LAUNCH + sizeof(double) * DDFG_FACETS_PER_LAUNCH +
                          sizeof(double) * (size_t)DDFG_FACETS_PER_LAUNCH * (size_t)acc_stride;
   const bool facet_inner = vs->single_vis_blocks && smem_fi <= 64 * 1024;
+  const bool block_fi = !vs->single_vis_blocks && smem_fi <= 64 * 1024;
   for (int f0 = 0; f0 < nfacets; f0 += DDFG_FACETS_PER_LAUNCH) {
     FacetPack pack;
     pack.n = min(DDFG_FACETS_PER_LAUNCH, nfacets - f0);
     for (int i = 0; i < pack.n; ++i) pack.f[i] = facets[f0 + i];
     const int npol = nvispol;
     cudaError_t e;
+    if (block_fi) {
+#define LAUNCH_B1(NP, SL)                                                                                          \
+  do {                                                                                                             \
+    if (smem_fi > 48 * 1024)                                                                                       \
+      cudaFuncSetAttribute(grid_block_fi_kernel<NP, SL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_fi); \
+    grid_block_fi_kernel<NP, SL><<<num_ctas, 256, smem_fi, stream>>>(*vs, *js, pack, gp, acc_stride);             \
+  } while (0)
+#define LAUNCH_B_NP(SL)              \
+  switch (npol) {                    \
+    case 1: LAUNCH_B1(1, SL); break; \
+    case 2: LAUNCH_B1(2, SL); break; \
+    case 3: LAUNCH_B1(3, SL); break; \
+    default: LAUNCH_B1(4, SL); break; \
+  }
+      if (slots == 2) { LAUNCH_B_NP(2) } else if (slots == 4) { LAUNCH_B_NP(4) } else { LAUNCH_B_NP(8) }
+#undef LAUNCH_B_NP
+#undef LAUNCH_B1
+      e = cudaGetLastError();
+      if (e != cudaSuccess) return ddfg_set_error(DDFG_ECUDA, "grid launch: %s", cudaGetErrorString(e));
+      continue;
+    }
     if (facet_inner) {
 #define LAUNCH_F1(NP, SL)                                                                                          \
   do {                                                                                                             \
