@@ -84,9 +84,11 @@ __global__ void __launch_bounds__(256) grid_kernel(const ddfg_vis vs, const ddfg
 // Averaged BDA blocks, facet-inner: each warp walks its 32 blocks for every facet of the launch
 // in turn (grid_block_record resets its Jones cache per block, so the order is free), so a
 // block's rows, visibilities, flags and weights are read from DRAM once per launch and from L1
-// for the other facets; per-facet shared accumulators hold the weight and Jones sums.
+// for the other facets; per-facet shared accumulators hold the weight and Jones sums.  The block
+// walk needs ~170 registers: CTAs of 128 threads, three per SM (12 warps; 256-thread CTAs at the
+// unconstrained 212 registers fit once, 8 warps).
 template <int NPOL, int SLOTS>
-__global__ void __launch_bounds__(256) grid_block_fi_kernel(const ddfg_vis vs, const ddfg_jones js,
+__global__ void __launch_bounds__(128, 3) grid_block_fi_kernel(const ddfg_vis vs, const ddfg_jones js,
                                                             const FacetPack pack, const GridParams gp,
                                                             int acc_stride) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -237,7 +239,7 @@ int ddfg_launch_grid(const ddfg_vis *vs, const ddfg_jones *js, const ddfg_facet 
   do {                                                                                                             \
     if (smem_fi > 48 * 1024)                                                                                       \
       cudaFuncSetAttribute(grid_block_fi_kernel<NP, SL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_fi); \
-    grid_block_fi_kernel<NP, SL><<<num_ctas, 256, smem_fi, stream>>>(*vs, *js, pack, gp, acc_stride);             \
+    grid_block_fi_kernel<NP, SL><<<2 * num_ctas, 128, smem_fi, stream>>>(*vs, *js, pack, gp, acc_stride);             \
   } while (0)
 #define LAUNCH_B_NP(SL)              \
   switch (npol) {                    \
