@@ -114,6 +114,7 @@ SIGNATURES = {
     "ddfg_stitch_facet": (C.c_int, [_vp, _i32, _i32, _i32, _vp, _vp, _vp, _vp, _vp, _i32, _i32, _i32, _vp]),
     "ddfg_image_normalise": (C.c_int, [_vp, _i32, _i32, _vp, _vp]),
     "ddfg_image_to_grid": (C.c_int, [_vp, _vp, _i32, _vp, _vp, _vp, _i32, _i32, _f64, _vp, _vp, _vp]),
+    "ddfg_image_to_grid_adjoint": (C.c_int, [_vp, _vp, _i32, _vp, _vp, _vp, _i32, _i32, _f64, _vp, _vp, _vp]),
 }
 
 _lock = threading.Lock()

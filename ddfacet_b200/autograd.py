@@ -9,6 +9,11 @@ subtract.  Its backward pass runs the library's hand-written adjoint kernels:
   phasor, J0^H g J1);
 * ``ddfg_degrid_jones_grad`` -- dLoss/dJ for the per-facet, per-antenna kMS Jones terms.
 
+``model_grids(fm, image)`` makes every facet's model grid from a model image (the facet machine's
+``image_to_facets``: crop, facet norm, spatial weight, taper correction, FFT) differentiably, its
+backward being ``ddfg_image_to_grid_adjoint``; composed with ``predict`` it gives the model image
+as a leaf tensor.
+
 Gradients follow PyTorch's complex convention (for a real loss, ``z.grad`` is
 dLoss/dRe z + i dLoss/dIm z).  Phases, smearing factors and Jones products are recomputed in the
 backward kernels from the same inputs rather than stored.  Supported: maps whose every block is
@@ -35,6 +40,12 @@ class PredictSetup:
     facets: List[D.FacetGrid]
     pol: object
     jones: Optional[D.JonesData] = None
+
+
+def setup_from_facet_machine(fm, vs: D.VisData, jones: Optional[D.JonesData] = None) -> PredictSetup:
+    """A prediction over every facet of a ``FacetMachine`` (its model facets' CF tables and
+    geometry, its polarisation)."""
+    return PredictSetup(vs=vs, facets=[f.model for f in fm.facets], pol=fm.pol, jones=jones)
 
 
 def _facets_with(setup: PredictSetup, grids: Sequence[torch.Tensor]):
@@ -94,3 +105,30 @@ def predict(setup: PredictSetup, model_grids: Sequence[torch.Tensor], jones_kms:
     if len(model_grids) != len(setup.facets):
         raise ValueError("one model grid per facet")
     return _Predict.apply(setup, jones_kms, *model_grids)
+
+
+class _ModelGrids(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, fm, image):
+        out = [torch.empty(f.model.grid.shape, dtype=torch.complex64, device=fm.device) for f in fm.facets]
+        fm.image_to_facets(image, out=out)
+        ctx.fm = fm
+        ctx.image_dtype = image.dtype
+        return tuple(out)
+
+    @staticmethod
+    def backward(ctx, *grads):
+        if not ctx.needs_input_grad[1]:
+            return None, None
+        g = ctx.fm.image_to_facets_adjoint(grads)
+        return None, g.to(ctx.image_dtype)
+
+
+def model_grids(fm, image: torch.Tensor) -> List[torch.Tensor]:
+    """Every facet's model grid (complex64 [nband, npol, N, N]) from the real model image
+    [nband, npol, M, M] of the facet machine ``fm``, differentiable with respect to the image."""
+    if image.dim() != 4 or tuple(image.shape) != (fm.nband, fm.npol, fm.npix_out, fm.npix_out):
+        raise ValueError(f"model image must be [{fm.nband}, {fm.npol}, {fm.npix_out}, {fm.npix_out}]")
+    if image.is_complex():
+        raise ValueError("the model image is real")
+    return list(_ModelGrids.apply(fm, image))

@@ -286,8 +286,6 @@ extern "C" int ddfg_degrid_adjoint(const ddfg_vis *vs, const ddfg_jones *js, con
   int policy = -1;
   int rc = degrid_checks(vs, js, pol, facets, nfacets, &policy);
   if (rc) return rc;
-  if (vs->nblocks > 0 && !vs->single_vis_blocks)
-    return ddfg_set_error(DDFG_EUNSUPPORTED, "degrid_adjoint: every block of the map must be one visibility");
   if (nfacets == 0 || vs->nblocks == 0) return DDFG_OK;
   return ddfg_launch_degrid_adjoint(vs, js, facets, nfacets, policy, pol->npol, ddfg_num_ctas(4),
                                     (cudaStream_t)stream);
@@ -299,8 +297,6 @@ extern "C" int ddfg_degrid_jones_grad(const ddfg_vis *vs, const ddfg_jones *js, 
   int policy = -1;
   int rc = degrid_checks(vs, js, pol, facets, nfacets, &policy);
   if (rc) return rc;
-  if (vs->nblocks > 0 && !vs->single_vis_blocks)
-    return ddfg_set_error(DDFG_EUNSUPPORTED, "degrid_jones_grad: every block of the map must be one visibility");
   if (js->mode == 0 || !js->kms || js->beam || js->interp_mode != 0 || !js->apply_amp || !js->apply_phase ||
       js->scale_jones)
     return ddfg_set_error(DDFG_EUNSUPPORTED,

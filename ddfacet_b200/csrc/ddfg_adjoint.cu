@@ -1,8 +1,8 @@
 // Backward passes of the degridder, for differentiating a visibility prediction.
 //
-// For single-visibility blocks the degridder's prediction of facet f at visibility v is linear
-// in the facet's model grid G_f:
-//     P_v = d ph_v J0 L(s) J1^H,   s_p = sum_t CF[t] G_f[p][cell_t],
+// The degridder's prediction of facet f at visibility v of block b is linear in the facet's
+// model grid G_f:
+//     P_v = d ph_v J0 L(s_b) J1^H,   s_b,p = sum_t CF[t] G_f[p][cell_t(b)],
 // with L the Stokes -> correlation map of the policy (Stokes.h:101-192), J0/J1 the antenna Jones
 // terms, ph_v = exp(+i nu angle) and d the smearing factor (degridder.h:202-261).  Given the
 // gradient g = dLoss/dP* of a real loss, the backward passes are:
@@ -11,7 +11,10 @@
 //     map (no 1/2 factors) and no weights;
 //   * Jones terms (J = J_kMS, nearest direction, no amplitude/phase normalisation): with
 //     Q = d ph L(s) J1^H and R = d ph J0 L(s), dLoss/dJ0* += g Q^H and dLoss/dJ1* += g^H R.
-// Phases, smearing and Jones terms are recomputed from the same inputs as the forward pass.
+// For averaged blocks the footprint is the block's (row means) and the adjoint value sums the
+// block's visibilities; with per-block Jones (BDAJones) J0, J1 are the block's middle-row pair and
+// the sums over the block come first.  Phases, smearing and Jones terms are recomputed from the
+// same inputs as the forward pass.
 #include <cuda_runtime.h>
 
 #include "ddfg_common.cuh"
@@ -79,6 +82,89 @@ __device__ __forceinline__ void adjoint_record(const DSingleIn &in, const ddfg_v
   for (int p = 0; p < NPOL; ++p) rec.stokes[p] = s[p];
   rec.valid = true;
   rec.gridchan = in.gridchan;
+}
+
+// The adjoint record of averaged block d on facet f: footprint by the degridder's block geometry
+// (row means, degridder.h:138-200), value L^H(J0m^H [sum over the block's visibilities of
+// d conj(ph) J0^H g J1] J1m) -- per-visibility Jones (mode 1) inside the sum, the per-block Jones
+// of the middle row and channel (mode 2) outside it, each looked up exactly as the forward pass
+// does (same cache, same walk order).
+template <int NPOL>
+__device__ __forceinline__ void adjoint_block_record(const DegridBlock &d, const ddfg_vis &vs, const ddfg_jones &js,
+                                                     const ddfg_facet &f, int policy, double n0m1,
+                                                     GridRecord<NPOL> &rec) {
+  rec.valid = false;
+  if (!degrid_block_geom(vs, f, d, rec.g)) return;
+  const int mid = d.rows[d.nrows / 2];
+  const float dec = (float)decorr_factor(vs, f, d.freqmean, mid);
+  JonesCache jc;
+  jc.reset();
+  M2 acc;
+#pragma unroll
+  for (int p = 0; p < 4; ++p) acc.v[p] = czero();
+  for (int inx = 0; inx < d.nrows; ++inx) {
+    const int64_t irow = d.rows[inx];
+    const double *up = vs.uvw + 3 * irow;
+    const double dot = up[0] * f.l0 + up[1] * f.m0 + up[2] * n0m1;
+    for (int ch = d.ch0; ch < d.ch1; ++ch) {
+      const float2 ph = cscale(phasor_turns(vs.freqs[ch] * dot * kInvC), dec);
+      M2 g = load_corr_matrix(vs, irow, ch);
+      if (js.mode == 1) {
+        jc.update(js, f.idir_kms, f.idir_beam, irow, ch, up[0], up[1]);
+        g = m2_times(m2_times(m2_herm(jc.j0), g), jc.j1);
+      }
+      g = m2_scale(g, cconj(ph));
+#pragma unroll
+      for (int p = 0; p < 4; ++p) acc.v[p] = cadd(acc.v[p], g.v[p]);
+    }
+  }
+  if (js.mode == 2) {
+    const double *up = vs.uvw + 3 * (int64_t)mid;
+    jc.update(js, f.idir_kms, f.idir_beam, mid, (d.ch0 + d.ch1) / 2, up[0], up[1]);
+    acc = m2_times(m2_times(m2_herm(jc.j0), acc), jc.j1);
+  }
+  float2 s[4];
+  stokes_adjoint<NPOL>(policy, acc, s);
+#pragma unroll
+  for (int p = 0; p < NPOL; ++p) rec.stokes[p] = s[p];
+  rec.valid = true;
+  rec.gridchan = d.gridchan;
+}
+
+// Averaged blocks: each lane walks its block per facet and the warp lays the 32 adjoint records
+// down with conjugated taps (the gridder's scatter).
+template <int NPOL, int SLOTS>
+__global__ void __launch_bounds__(256) degrid_adjoint_block_kernel(const ddfg_vis vs, const ddfg_jones js,
+                                                                   const FacetPack pack, int policy) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  ddfg_facet *sf = (ddfg_facet *)smem_raw;
+  double *s_n0m1 = (double *)(sf + DDFG_FACETS_PER_LAUNCH);
+  stage_facets(pack, sf);
+  __syncthreads();
+  if (threadIdx.x < pack.n) {
+    const ddfg_facet &f = sf[threadIdx.x];
+    s_n0m1[threadIdx.x] = sqrt(1. - f.l0 * f.l0 - f.m0 * f.m0) - 1.;
+  }
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  const int warp = threadIdx.x >> 5;
+  const int nwarps = blockDim.x >> 5;
+  const int64_t nstripes = (vs.nblocks + 31) / 32;
+  LaneTaps<SLOTS> lt;
+  lt.reset();
+  for (int64_t s = (int64_t)blockIdx.x * nwarps + warp; s < nstripes; s += (int64_t)gridDim.x * nwarps) {
+    const int64_t b = s * 32 + lane;
+    const bool inrange = b < vs.nblocks;
+    DegridBlock d;
+    if (inrange) degrid_block_header(vs, b, d);
+    for (int fi = 0; fi < pack.n; ++fi) {
+      const ddfg_facet &f = sf[fi];
+      GridRecord<NPOL> rec;
+      rec.valid = false;
+      if (inrange) adjoint_block_record<NPOL>(d, vs, js, f, policy, s_n0m1[fi], rec);
+      scatter_records<NPOL, SLOTS, true>(rec, f, min(NPOL, f.npol), lt, lane);
+    }
+  }
 }
 
 template <int NPOL, int SLOTS>
@@ -187,6 +273,112 @@ __global__ void __launch_bounds__(256) jones_grad_kernel(const ddfg_vis vs, cons
   }
 }
 
+__device__ __forceinline__ size_t kms_offset(const ddfg_jones &js, int t, int dir, int a, int c) {
+  const size_t nd = (size_t)js.kms_dims[1], na = (size_t)js.kms_dims[2], nch = (size_t)js.kms_dims[3];
+  return (((size_t)t * nd + (size_t)dir) * na + (size_t)a) * nch * 4 + (size_t)c * 4;
+}
+
+__device__ __forceinline__ M2 load_m2(const float2 *J, size_t o) {
+  M2 m;
+#pragma unroll
+  for (int p = 0; p < 4; ++p) m.v[p] = J[o + p];
+  return m;
+}
+
+// dLoss/dJ_kMS* for averaged blocks: the block's model sample M = L(s) is gathered once per facet;
+// per visibility (mode 1) g Q^H and g^H R are reduced into the visibility's Jones cells, or
+// (mode 2, one Jones pair per block at its middle row and channel) G (M J1^H)^H and
+// G^H J0 M with G = sum over the block of d conj(ph) g.
+template <int NPOL, int SLOTS>
+__global__ void __launch_bounds__(256) jones_grad_block_kernel(const ddfg_vis vs, const ddfg_jones js,
+                                                               const FacetPackD pack, int policy, float2 *grad) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  ddfg_facet *sf = (ddfg_facet *)smem_raw;
+  double *s_n0m1 = (double *)(sf + DDFG_FACETS_PER_LAUNCH);
+  float2 *partial = (float2 *)(s_n0m1 + DDFG_FACETS_PER_LAUNCH);
+  stage_facets(pack, sf);
+  __syncthreads();
+  if (threadIdx.x < pack.n) {
+    const ddfg_facet &f = sf[threadIdx.x];
+    s_n0m1[threadIdx.x] = sqrt(1. - f.l0 * f.l0 - f.m0 * f.m0) - 1.;
+  }
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  const int warp = threadIdx.x >> 5;
+  const int nwarps = blockDim.x >> 5;
+  const int64_t nstripes = (vs.nblocks + 31) / 32;
+  float2 *wpart = partial + warp * 32 * 32;
+  LaneTaps<SLOTS> lt;
+  lt.reset();
+  const float2 *J = (const float2 *)js.kms;
+  for (int64_t s = (int64_t)blockIdx.x * nwarps + warp; s < nstripes; s += (int64_t)gridDim.x * nwarps) {
+    const int64_t b = s * 32 + lane;
+    const bool inrange = b < vs.nblocks;
+    DegridBlock d;
+    if (inrange) degrid_block_header(vs, b, d);
+    for (int fi = 0; fi < pack.n; ++fi) {
+      const ddfg_facet &f = sf[fi];
+      BlockGeom geo;
+      const bool valid = inrange && degrid_block_geom(vs, f, d, geo);
+      TapJob job;
+      if (valid) job = tap_job(geo, d.gridchan, f);
+      float2 mine[NPOL];
+      gather_records<NPOL, SLOTS>(valid, job, f, lt, wpart, lane, mine);
+      if (!valid) continue;
+      float2 sv[4];
+#pragma unroll
+      for (int p = 0; p < 4; ++p) sv[p] = (p < NPOL) ? mine[p] : czero();
+      const M2 m = corr_from_stokes(policy, sv);
+      const int mid = d.rows[d.nrows / 2];
+      const float dec = (float)decorr_factor(vs, f, d.freqmean, mid);
+      M2 G;
+#pragma unroll
+      for (int p = 0; p < 4; ++p) G.v[p] = czero();
+      for (int inx = 0; inx < d.nrows; ++inx) {
+        const int64_t irow = d.rows[inx];
+        const double *up = vs.uvw + 3 * irow;
+        const double dot = up[0] * f.l0 + up[1] * f.m0 + up[2] * s_n0m1[fi];
+        for (int ch = d.ch0; ch < d.ch1; ++ch) {
+          const float2 ph = cscale(phasor_turns(vs.freqs[ch] * dot * kInvC), dec);
+          const M2 g = load_corr_matrix(vs, irow, ch);
+          if (js.mode == 1) {
+            const JonesIdx x = jones_idx(js, irow, ch);
+            const size_t o0 = kms_offset(js, x.tk, f.idir_kms, x.a0, x.ck);
+            const size_t o1 = kms_offset(js, x.tk, f.idir_kms, x.a1, x.ck);
+            const M2 j0 = load_m2(J, o0), j1 = load_m2(J, o1);
+            const M2 q = m2_scale(m2_times(m, m2_herm(j1)), ph);  // d ph L(s) J1^H
+            const M2 r = m2_scale(m2_times(j0, m), ph);           // d ph J0 L(s)
+            const M2 d0 = m2_times(g, m2_herm(q));
+            const M2 d1 = m2_times(m2_herm(g), r);
+#pragma unroll
+            for (int p = 0; p < 4; ++p) {
+              red_add(grad + o0 + p, d0.v[p]);
+              red_add(grad + o1 + p, d1.v[p]);
+            }
+          } else {
+            const M2 gp = m2_scale(g, cconj(ph));
+#pragma unroll
+            for (int p = 0; p < 4; ++p) G.v[p] = cadd(G.v[p], gp.v[p]);
+          }
+        }
+      }
+      if (js.mode == 2) {
+        const JonesIdx x = jones_idx(js, mid, (d.ch0 + d.ch1) / 2);
+        const size_t o0 = kms_offset(js, x.tk, f.idir_kms, x.a0, x.ck);
+        const size_t o1 = kms_offset(js, x.tk, f.idir_kms, x.a1, x.ck);
+        const M2 j0 = load_m2(J, o0), j1 = load_m2(J, o1);
+        const M2 d0 = m2_times(G, m2_herm(m2_times(m, m2_herm(j1))));
+        const M2 d1 = m2_times(m2_herm(G), m2_times(j0, m));
+#pragma unroll
+        for (int p = 0; p < 4; ++p) {
+          red_add(grad + o0 + p, d0.v[p]);
+          red_add(grad + o1 + p, d1.v[p]);
+        }
+      }
+    }
+  }
+}
+
 }  // namespace ddfg
 
 using namespace ddfg;
@@ -201,7 +393,13 @@ int ddfg_launch_degrid_adjoint(const ddfg_vis *vs, const ddfg_jones *js, const d
     FacetPack pack;
     pack.n = min(DDFG_FACETS_PER_LAUNCH, nfacets - f0);
     for (int i = 0; i < pack.n; ++i) pack.f[i] = facets[f0 + i];
-#define LAUNCH_A(NP, SL) degrid_adjoint_kernel<NP, SL><<<num_ctas, 256, smem, stream>>>(*vs, *js, pack, policy)
+#define LAUNCH_A(NP, SL)                                                                      \
+  do {                                                                                        \
+    if (vs->single_vis_blocks)                                                                \
+      degrid_adjoint_kernel<NP, SL><<<num_ctas, 256, smem, stream>>>(*vs, *js, pack, policy);       \
+    else                                                                                      \
+      degrid_adjoint_block_kernel<NP, SL><<<num_ctas, 256, smem, stream>>>(*vs, *js, pack, policy); \
+  } while (0)
 #define LAUNCH_A_NP(SL)              \
   switch (nvispol) {                 \
     case 1: LAUNCH_A(1, SL); break;  \
@@ -230,10 +428,16 @@ int ddfg_launch_jones_grad(const ddfg_vis *vs, const ddfg_jones *js, const ddfg_
     FacetPackD pack;
     pack.n = min(DDFG_FACETS_PER_LAUNCH, nfacets - f0);
     for (int i = 0; i < pack.n; ++i) pack.f[i] = facets[f0 + i];
-#define LAUNCH_J(NP, SL)                                                                                      \
-  do {                                                                                                        \
-    cudaFuncSetAttribute(jones_grad_kernel<NP, SL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);  \
-    jones_grad_kernel<NP, SL><<<num_ctas, 256, smem, stream>>>(*vs, *js, pack, policy, g);                    \
+#define LAUNCH_J(NP, SL)                                                                                   \
+  do {                                                                                                     \
+    if (vs->single_vis_blocks) {                                                                           \
+      cudaFuncSetAttribute(jones_grad_kernel<NP, SL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem); \
+      jones_grad_kernel<NP, SL><<<num_ctas, 256, smem, stream>>>(*vs, *js, pack, policy, g);                 \
+    } else {                                                                                               \
+      cudaFuncSetAttribute(jones_grad_block_kernel<NP, SL>, cudaFuncAttributeMaxDynamicSharedMemorySize,     \
+                           (int)smem);                                                                     \
+      jones_grad_block_kernel<NP, SL><<<num_ctas, 256, smem, stream>>>(*vs, *js, pack, policy, g);           \
+    }                                                                                                      \
   } while (0)
 #define LAUNCH_J_NP(SL)              \
   switch (nvispol) {                 \

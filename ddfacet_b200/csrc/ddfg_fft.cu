@@ -145,6 +145,32 @@ __global__ void model_gather_kernel(const float *__restrict__ image, int planes,
   }
 }
 
+// The adjoint of model_gather_kernel with respect to the real image, accumulated:
+// grad[p][x0m + a][y0m + c] += scale * Re(work[p][(i - h) mod n][(j - h) mod n]) * coef(pr, pc)
+// with pr = x0f + a, pc = y0f + c, (i, j) = (n-1-pc, pr) and coef = sw / sphe / norm (0 where
+// sphe < 1e-3): every image pixel of the facet box reads the one grid cell its value went to.
+__global__ void model_gather_adjoint_kernel(const float2 *__restrict__ work, int planes, int m,
+                                            const float *__restrict__ norm, const float *__restrict__ sw,
+                                            const float *__restrict__ sphe, int n, Edges e, float scale,
+                                            float *__restrict__ grad) {
+  const int h = n / 2;
+  const int wa = e.x1m - e.x0m, wb = e.y1m - e.y0m;
+  const int64_t per = (int64_t)wa * wb, total = per * planes, nn = (int64_t)n * n;
+  for (int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
+       idx += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t p = idx / per;
+    const int64_t k = idx - p * per;
+    const int a = (int)(k / wb), c = (int)(k - (int64_t)a * wb);
+    const int pr = e.x0f + a, pc = e.y0f + c;
+    const float s = sphe[(int64_t)pr * n + pc];
+    if (s < 1e-3f) continue;
+    const int y = wrap(n - 1 - pc, n - h, n), x = wrap(pr, n - h, n);
+    const int64_t mi = (int64_t)(e.x0m + a) * m + (e.y0m + c);
+    const float v = work[p * nn + (int64_t)y * n + x].x * scale;
+    grad[p * (int64_t)m * m + mi] += v / norm[mi] * sw[(int64_t)pr * n + pc] / s;
+  }
+}
+
 int nctas_for(int64_t total) {
   const int64_t b = (total + 255) / 256;
   const int64_t cap = ddfg_num_ctas(8);
@@ -250,5 +276,32 @@ extern "C" int ddfg_image_to_grid(ddfg_fft_plan *p, const float *image, int32_t 
                                                              (float)(1.0 / ((double)n * n)));
   cudaError_t err = cudaGetLastError();
   if (err != cudaSuccess) return ddfg_set_error(DDFG_ECUDA, "image_to_grid: %s", cudaGetErrorString(err));
+  return DDFG_OK;
+}
+
+extern "C" int ddfg_image_to_grid_adjoint(ddfg_fft_plan *p, const void *grid_grad, int32_t m, const float *norm_image,
+                                          const float *sw_img, const float *sphe, int32_t xc, int32_t yc,
+                                          double overs, float *image_grad, void *work, void *stream_) {
+  cudaStream_t stream = (cudaStream_t)stream_;
+  if (!p || !grid_grad || !norm_image || !sw_img || !sphe || !image_grad || !work || m <= 0)
+    return ddfg_set_error(DDFG_EINVAL, "image_to_grid_adjoint: bad argument");
+  const int n = p->n;
+  const Edges e = give_edges(xc, yc, m, n);
+  if (e.x1m <= e.x0m || e.y1m <= e.y0m) return DDFG_OK;  // facet box outside the image
+  const int64_t total = (int64_t)p->batch * n * n;
+  // adjoint of (fftshift, times 1/N^2): ifftshift, times 1/N^2
+  ishift_scale_kernel<<<nctas_for(total), 256, 0, stream>>>((const float2 *)grid_grad, (float2 *)work, n, p->batch,
+                                                              (float)(1.0 / ((double)n * n)));
+  if (cufftSetStream(p->h, stream) != CUFFT_SUCCESS)
+    return ddfg_set_error(DDFG_ECUDA, "image_to_grid_adjoint: cufftSetStream");
+  // adjoint of the unnormalised forward DFT: the unnormalised inverse DFT
+  if (cufftExecC2C(p->h, (cufftComplex *)work, (cufftComplex *)work, CUFFT_INVERSE) != CUFFT_SUCCESS)
+    return ddfg_set_error(DDFG_ECUDA, "image_to_grid_adjoint: cufftExecC2C failed");
+  const double s = overs * (double)n;
+  const int64_t pix = (int64_t)(e.x1m - e.x0m) * (e.y1m - e.y0m) * p->batch;
+  model_gather_adjoint_kernel<<<nctas_for(pix), 256, 0, stream>>>((const float2 *)work, p->batch, m, norm_image,
+                                                                    sw_img, sphe, n, e, (float)(s * s), image_grad);
+  cudaError_t err = cudaGetLastError();
+  if (err != cudaSuccess) return ddfg_set_error(DDFG_ECUDA, "image_to_grid_adjoint: %s", cudaGetErrorString(err));
   return DDFG_OK;
 }

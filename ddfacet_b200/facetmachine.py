@@ -21,7 +21,7 @@ from __future__ import annotations
 
 import ctypes as C
 from dataclasses import dataclass
-from typing import List, Optional
+from typing import List, Optional, Sequence
 
 import numpy as np
 import torch
@@ -256,21 +256,52 @@ class FacetMachine:
             norm = torch.where(norm == 0, torch.ones_like(norm), norm)
         return (sw * torch.sqrt(norm)[:, None]).contiguous()
 
-    def image_to_facets(self, model_image: torch.Tensor, stream=None):
+    def image_to_facets(self, model_image: torch.Tensor, stream=None, out: Optional[List[torch.Tensor]] = None):
         """Every facet's model grid from the model image float32 [nband, npol, M, M]
-        (``set_model_grid`` with ``GiveModelTessel(ToGrid=True)``)."""
+        (``set_model_grid`` with ``GiveModelTessel(ToGrid=True)``), written into the facets' model
+        grids or into ``out`` (one complex64 [nband, npol, N, N] tensor per facet)."""
         lib = _abi.lib()
         st = D._stream_ptr(stream)
         img = model_image.to(self.device, torch.float32).contiguous()
         m = img.shape[-1]
-        for f in self.facets:
+        targets = [f.model.grid for f in self.facets] if out is None else out
+        if len(targets) != len(self.facets):
+            raise ValueError("one output grid per facet")
+        for f, g in zip(self.facets, targets):
             n = f.model.grid.shape[-1]
+            if g.shape != f.model.grid.shape or g.dtype != torch.complex64 or not g.is_contiguous():
+                raise ValueError(f"output grid must be contiguous complex64 {tuple(f.model.grid.shape)}")
             xc, yc = f.geom.pix_central
             _abi.check(lib.ddfg_image_to_grid(self._plan(n), C.c_void_p(img.data_ptr()), m,
                                               C.c_void_p(self.facet_norm.data_ptr()), C.c_void_p(f.sw_img.data_ptr()),
                                               C.c_void_p(f.sphe.data_ptr()), xc, yc, C.c_double(float(self.overs)),
-                                              C.c_void_p(f.model.grid.data_ptr()),
-                                              C.c_void_p(self._work_for(n).data_ptr()), st))
+                                              C.c_void_p(g.data_ptr()), C.c_void_p(self._work_for(n).data_ptr()), st))
+
+    def image_to_facets_adjoint(self, grid_grads: Sequence[torch.Tensor], stream=None) -> torch.Tensor:
+        """The adjoint of ``image_to_facets`` with respect to the real model image: the gradient
+        float32 [nband, npol, M, M] of a real loss given its gradients with respect to every facet's
+        model grid (PyTorch's complex convention), summed over facets."""
+        lib = _abi.lib()
+        st = D._stream_ptr(stream)
+        m = self.npix_out
+        if len(grid_grads) != len(self.facets):
+            raise ValueError("one grid gradient per facet")
+        grad = torch.zeros((self.nband, self.npol, m, m), dtype=torch.float32, device=self.device)
+        for f, g in zip(self.facets, grid_grads):
+            if g is None:
+                continue
+            n = f.model.grid.shape[-1]
+            g = g.to(self.device, torch.complex64).contiguous()
+            if g.shape != f.model.grid.shape:
+                raise ValueError(f"grid gradient must have shape {tuple(f.model.grid.shape)}")
+            xc, yc = f.geom.pix_central
+            _abi.check(lib.ddfg_image_to_grid_adjoint(self._plan(n), C.c_void_p(g.data_ptr()), m,
+                                                      C.c_void_p(self.facet_norm.data_ptr()),
+                                                      C.c_void_p(f.sw_img.data_ptr()), C.c_void_p(f.sphe.data_ptr()),
+                                                      xc, yc, C.c_double(float(self.overs)),
+                                                      C.c_void_p(grad.data_ptr()),
+                                                      C.c_void_p(self._work_for(n).data_ptr()), st))
+        return grad
 
 
 def _edges(xc, yc, m, n):

@@ -169,17 +169,18 @@ int ddfg_degrid(const ddfg_vis *vs, const ddfg_jones *js, const ddfg_pol *pol,
  * complex64 [nrow][nchan][ncorr], read only), this adds P's adjoint applied to it to each
  * facets[i].grid (+=): conj(CF) taps at the degridder's footprint, the adjoint Stokes map (for
  * Stokes I from XX/YY: g_XX + g_YY), conj(phasor), J0^H g J1 and the smearing factor.  The
- * facets carry the degridder's CF order (as for ddfg_degrid).  Maps whose every block is one
- * visibility only (DDFG_EUNSUPPORTED otherwise).  No counterpart in the reference, whose
- * degridder has no derivative. */
+ * facets carry the degridder's CF order (as for ddfg_degrid).  Averaged BDA blocks sum their
+ * visibilities' back-projected gradients at the block's footprint; per-block Jones (BDAJones)
+ * are applied to that sum.  No counterpart in the reference, whose degridder has no
+ * derivative. */
 int ddfg_degrid_adjoint(const ddfg_vis *vs, const ddfg_jones *js, const ddfg_pol *pol,
                         const ddfg_facet *facets, int nfacets, void *stream);
 
 /* Backward pass of ddfg_degrid for the kMS Jones terms: with vs->vis = dLoss/dP* as above and
  * facets[i].grid the model grids of the forward pass, adds dLoss/dJ* to grad_kms (complex64,
  * the layout of js->kms, +=).  Needs kMS Jones only, nearest direction, no amplitude/phase
- * normalisation, single-visibility blocks (DDFG_EUNSUPPORTED otherwise).  No counterpart in the
- * reference. */
+ * normalisation (DDFG_EUNSUPPORTED otherwise); any BDA map, per-visibility or per-block
+ * (BDAJones) Jones.  No counterpart in the reference. */
 int ddfg_degrid_jones_grad(const ddfg_vis *vs, const ddfg_jones *js, const ddfg_pol *pol,
                            const ddfg_facet *facets, int nfacets, void *grad_kms, void *stream);
 
@@ -309,6 +310,16 @@ int ddfg_image_normalise(float *image, int32_t planes, int32_t m, const float *f
 int ddfg_image_to_grid(ddfg_fft_plan *plan, const float *image, int32_t m, const float *norm_image,
                        const float *sw_img, const float *sphe, int32_t xc, int32_t yc, double overs, void *grid_out,
                        void *work, void *stream);
+
+/* The adjoint of ddfg_image_to_grid with respect to the (real) model image, for differentiating a
+ * prediction through the model image (no reference counterpart: the reference has no derivative).
+ * image_grad float32 [batch][M][M] += Re(A^H grid_grad) where A is ddfg_image_to_grid's linear map
+ * with the same arguments; grid_grad is complex64 [batch][N][N] (PyTorch's gradient convention).
+ * Pixels outside the facet's GiveEdges box or where sphe < 1e-3 receive nothing.  work: a
+ * [batch][N][N] complex64 scratch buffer. */
+int ddfg_image_to_grid_adjoint(ddfg_fft_plan *plan, const void *grid_grad, int32_t m, const float *norm_image,
+                               const float *sw_img, const float *sphe, int32_t xc, int32_t yc, double overs,
+                               float *image_grad, void *work, void *stream);
 
 #ifdef __cplusplus
 }

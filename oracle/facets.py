@@ -6,7 +6,10 @@ NumPy, so the GPU kernels (cuFFT + fused passes) can be compared with it:
                            FFTW_2Donly_np.ifft (ModFFTW.py:631-648);
   * facets_to_im_channel-- ClassFacetMachine.FacetsToIm_Channel (ClassFacetMachine.py:1331-1416);
   * give_model_tessel   -- ClassImToGrid.GiveModelTessel(ToGrid=True) (ClassImToGrid.py:138-264)
-                           with FFTW_2Donly_np.fft (ModFFTW.py:611-629).
+                           with FFTW_2Donly_np.fft (ModFFTW.py:611-629);
+  * give_model_tessel_adjoint -- the adjoint of give_model_tessel with respect to the real model
+                           image (no reference counterpart), each step of the forward undone in
+                           reverse order in float64.
 """
 import numpy as np
 
@@ -83,4 +86,25 @@ def give_model_tessel(image, norm_im, sphe, sw_img, xc, yc, n, overs):
             b = np.fft.ifftshift(model[ch, pol].astype(np.complex128))
             b = np.fft.fft2(b)
             out[ch, pol] = np.fft.fftshift(b) / (n * n)
+    return out
+
+
+def give_model_tessel_adjoint(grid_grad, norm_im, sphe, sw_img, xc, yc, npix_out, overs):
+    """Re(A^H y) for A = give_model_tessel(., norm_im, sphe, sw_img, xc, yc, n, overs) acting on a
+    real image [nch, npol, M, M]; y is complex [nch, npol, n, n]. Returns float64 [nch, npol, M, M]."""
+    y = np.asarray(grid_grad, np.complex128)
+    nch, npol, n, _ = y.shape
+    (x0d, x1d, y0d, y1d), (x0p, x1p, y0p, y1p) = give_edges(xc, yc, npix_out, n)
+    out = np.zeros((nch, npol, npix_out, npix_out), np.float64)
+    mask = np.asarray(sphe) < 1e-3
+    for ch in range(nch):
+        for pol in range(npol):
+            b = np.fft.ifftshift(y[ch, pol]) / (n * n)       # adjoint of fftshift(.) / n^2
+            b = np.fft.ifft2(b) * (n * n)                    # adjoint of the unnormalised fft2
+            b = np.fft.fftshift(b) * float(overs * n) ** 2   # adjoint of ifftshift, then the scale
+            b = b[::-1, :].T                                 # adjoint of .T[::-1, :]
+            b = np.where(mask, 0, b.real)
+            box = b[x0p:x1p, y0p:y1p] / np.asarray(norm_im, np.float64)[x0d:x1d, y0d:y1d]
+            box = box * np.asarray(sw_img, np.float64)[x0p:x1p, y0p:y1p] / np.asarray(sphe, np.float64)[x0p:x1p, y0p:y1p]
+            out[ch, pol, x0d:x1d, y0d:y1d] += box
     return out

@@ -25,13 +25,21 @@ pytestmark = pytest.mark.gpu
 LMS = [(0.004, -0.002), (-0.006, 0.005)]
 
 
-def _setup(jones=True):
-    cs = [cases.make_case(seed=17, nant=8, ntimes=12, nchan=8, ncorr=4, stokes_ids=(1,), nw=3, lm=lm) for lm in LMS]
+# maps: "single" (every block one visibility) or "bda" (DDFacet's mode-1 map with averaged blocks)
+MAPS = {"single": {}, "bda": dict(bda_mode=1, dphi=np.sqrt(6 * 0.05))}
+
+
+def _setup(jones=True, kind="single", jones_mode=1):
+    cs = [cases.make_case(seed=17, nant=8, ntimes=12, nchan=8, ncorr=4, stokes_ids=(1,), nw=3, lm=lm, **MAPS[kind])
+          for lm in LMS]
     for c in cs[1:]:
         c.vis = cs[0].vis
+    if kind == "bda":
+        nb = int(np.uint32(cs[0].bda[0]))
+        assert cs[0].nrow * cs[0].nchan / nb > 1.5  # the blocks do average
     if jones:
         for i, c in enumerate(cs):
-            cases.add_jones(c, mode=1, nt=3, nd=3, idir=i + 1)
+            cases.add_jones(c, mode=jones_mode, nt=3, nd=3, idir=i + 1)
     objs = [cases._gpu_objs(c) for c in cs]
     setup = PredictSetup(vs=objs[0][0], facets=[o[1] for o in objs], pol=D.make_pol(cs[0].corr_ids, [1]),
                          jones=objs[0][2])
@@ -50,8 +58,9 @@ def _vdot(a, b):
     return complex(torch.sum(torch.conj(a.to(torch.complex128)) * b.to(torch.complex128)).item())
 
 
-def test_dot_product_adjoint():
-    cs, setup = _setup(jones=True)
+@pytest.mark.parametrize("kind,jones_mode", [("single", 1), ("bda", 1), ("bda", 2)])
+def test_dot_product_adjoint(kind, jones_mode):
+    cs, setup = _setup(jones=True, kind=kind, jones_mode=jones_mode)
     rng = np.random.default_rng(0)
     kms = setup.jones.kms
     errs = []
@@ -64,7 +73,7 @@ def test_dot_product_adjoint():
         lhs = _vdot(y, P.detach())
         rhs = sum(_vdot(g, xi.detach()) for g, xi in zip(gx, x))
         errs.append(abs(lhs - rhs) / abs(lhs))
-    print(f"dot-product test: mean rel {np.mean(errs):.2e}  max {np.max(errs):.2e}")
+    print(f"dot-product test ({kind}, Jones mode {jones_mode}): mean rel {np.mean(errs):.2e}  max {np.max(errs):.2e}")
     assert np.mean(errs) < 1e-6 and np.max(errs) < 1e-5
 
 
@@ -91,8 +100,9 @@ def _gpu_loss_grads(setup, grids, kms, V, w):
     return [xi.grad.cpu().numpy() for xi in x], k.grad.cpu().numpy(), P.detach().cpu().numpy()
 
 
-def test_finite_differences_fp64():
-    cs, setup = _setup(jones=True)
+@pytest.mark.parametrize("kind,jones_mode", [("single", 1), ("bda", 1), ("bda", 2)])
+def test_finite_differences_fp64(kind, jones_mode):
+    cs, setup = _setup(jones=True, kind=kind, jones_mode=jones_mode)
     rng = np.random.default_rng(1)
     grids = [g.cpu().numpy() * np.float32(0.01) for g in _rand_grids(setup, rng)]
     kms = np.ascontiguousarray(cs[0].jones["kms"], np.complex64)
@@ -136,7 +146,8 @@ def test_finite_differences_fp64():
     fd, an = np.array(fd), np.array(an)
     ej = np.linalg.norm(fd[:32] - an[:32]) / np.linalg.norm(fd[:32])
     eg = np.linalg.norm(fd[32:] - an[32:]) / np.linalg.norm(fd[32:])
-    print(f"finite differences (FP64 oracle) vs GPU gradient: Jones {ej:.2e}  grid {eg:.2e}")
+    print(f"finite differences (FP64 oracle, {kind}, Jones mode {jones_mode}) vs GPU gradient: "
+          f"Jones {ej:.2e}  grid {eg:.2e}")
     assert ej < 1e-4 and eg < 1e-4
 
 
@@ -157,11 +168,141 @@ def test_adjoint_matches_reference_gridder_on_residuals():
         assert e < 1e-4
 
 
-def test_unsupported_maps_raise():
-    c = cases.make_case(seed=3, bda_mode=1, dphi=np.sqrt(6 * 0.05), nchan=8)
+def test_unsupported_jones_gradient_raises():
+    """The Jones gradient covers kMS Jones at the nearest direction without normalisation; weighted
+    directions are refused with the library's message (the model-grid gradient still works)."""
+    c = cases.make_case(seed=3, bda_mode=1, dphi=np.sqrt(6 * 0.05), nchan=8, ncorr=4)
+    cases.add_jones(c, mode=1, nt=3, nd=3, interp_mode=1)
     vs, fg, jd = cases._gpu_objs(c)
-    setup = PredictSetup(vs=vs, facets=[fg], pol=D.make_pol(c.corr_ids, c.stokes_ids), jones=None)
+    setup = PredictSetup(vs=vs, facets=[fg], pol=D.make_pol(c.corr_ids, c.stokes_ids), jones=jd)
     x = torch.zeros_like(fg.grid).requires_grad_(True)
-    P = predict(setup, [x])
-    with pytest.raises(ValueError, match="one visibility"):
-        P.abs().sum().backward()
+    (gx,) = torch.autograd.grad(predict(setup, [x], jd.kms).abs().sum(), [x])
+    assert gx.shape == x.shape
+    k = jd.kms.clone().requires_grad_(True)
+    P = predict(setup, [x.detach()], k)
+    with pytest.raises(ValueError, match="nearest direction"):
+        torch.autograd.grad(P.real.sum(), [k])
+
+
+# ---- the model image as the leaf: image -> facet grids (crop, norm, taper, FFT) -> prediction ----
+
+def _image_problem(kind, seed=21):
+    from ddfacet_b200 import bda, geometry, synth
+    from ddfacet_b200.facetmachine import FacetMachine
+
+    npix = 600
+    obs = synth.make_observation(seed, 8, 2000.0, 34.0, 40.0, 12 * 30.0 / 3600.0, 30.0, 8, 1.30e9, 1.45e9)
+    wmax = float(np.max(np.abs(obs.uvw[:, 2]))) * 1.01
+    tess = None
+    if kind == "voronoi":
+        r = npix * 6.0 / 3600 * np.pi / 180 / 2
+        rng = np.random.default_rng(seed)
+        tess = geometry.voronoi_facets(npix, 6.0, rng.uniform(-0.8 * r, 0.8 * r, 4), rng.uniform(-0.8 * r, 0.8 * r, 4),
+                                       1.7)
+    fm = FacetMachine(npix, 6.0, 2, obs.freqs, padding=1.7, nband=1, stokes_ids=(1,), corr_ids=(9, 10, 11, 12),
+                      support=7, nw=3, wmax=wmax, mixing_width=10.0, tessellation=tess)
+    dev = fm.device
+    vis = np.zeros((obs.nrow, obs.freqs.size, 4), np.complex64)
+    vs = D.VisData.create(vis, obs.uvw, np.zeros(vis.shape, bool), np.ones((obs.nrow, obs.freqs.size), np.float32),
+                          obs.freqs, np.zeros(obs.freqs.size, np.int32), bda.plain_map(obs.A0, obs.A1, obs.freqs.size),
+                          device=dev)
+    nd = len(fm.facets)
+    t = obs.times
+    tmap = np.minimum(((t - t.min()) / (t.max() - t.min() + 1e-9) * 3).astype(np.int32), 2)
+    kms = torch.from_numpy(synth.random_jones(seed + 1, 3, nd, obs.nant, 1, 0.1)).to(dev)
+    jd = D.JonesData(mode=1, kms=kms, kms_tmap=torch.from_numpy(tmap).to(dev),
+                     kms_cmap=torch.zeros(obs.freqs.size, dtype=torch.int32, device=dev),
+                     a0=torch.from_numpy(obs.A0.astype(np.int32)).to(dev),
+                     a1=torch.from_numpy(obs.A1.astype(np.int32)).to(dev),
+                     wavelength_mean=float(np.mean(299792458.0 / obs.freqs)))
+    return fm, vs, jd
+
+
+@pytest.mark.parametrize("kind", ["regular", "voronoi"])
+def test_image_to_grid_adjoint_matches_oracle(kind):
+    """ddfg_image_to_grid_adjoint summed over facets against the FP64 restatement of the adjoint
+    (oracle/facets.py give_model_tessel_adjoint): 1e-5 relative RMS."""
+    from oracle import facets as OF
+
+    fm, _, _ = _image_problem(kind)
+    rng = np.random.default_rng(3)
+    ys = [torch.from_numpy((rng.standard_normal(f.model.grid.shape) + 1j * rng.standard_normal(f.model.grid.shape))
+                           .astype(np.complex64)).cuda() for f in fm.facets]
+    got = fm.image_to_facets_adjoint(ys).cpu().numpy()
+    want = np.zeros(got.shape, np.float64)
+    for f, y in zip(fm.facets, ys):
+        want += OF.give_model_tessel_adjoint(y.cpu().numpy(), fm.facet_norm_host, f.sphe.cpu().numpy(), f.sw_host,
+                                             *f.geom.pix_central, fm.npix_out, fm.overs)
+    e = cases.rel_rms(got, want)
+    print(f"image adjoint vs FP64 oracle ({kind}): {e:.2e}")
+    assert e < 1e-5
+
+
+def test_image_leaf_dot_product_256_pairs():
+    """Re <y, P(x)> = <x, grad> for the whole chain real image x -> facet grids -> prediction with
+    per-facet Jones, over 256 random pairs: relative difference <= 1e-6 in the mean, 1e-5 for any
+    pair (float64 inner products of the float32 results)."""
+    from ddfacet_b200.autograd import model_grids, predict, setup_from_facet_machine
+
+    fm, vs, jd = _image_problem("voronoi")
+    setup = setup_from_facet_machine(fm, vs, jd)
+    rng = np.random.default_rng(5)
+    shape = (fm.nband, fm.npol, fm.npix_out, fm.npix_out)
+    errs = []
+    for _ in range(256):
+        x = torch.from_numpy(rng.standard_normal(shape).astype(np.float32)).cuda().requires_grad_(True)
+        y = torch.from_numpy((rng.standard_normal(vs.vis.shape) + 1j * rng.standard_normal(vs.vis.shape))
+                             .astype(np.complex64)).cuda()
+        P = predict(setup, model_grids(fm, x), jd.kms)
+        (gx,) = torch.autograd.grad(P, [x], grad_outputs=y)
+        lhs = _vdot(y, P.detach()).real
+        rhs = float(torch.sum(gx.double() * x.detach().double()).item())
+        errs.append(abs(lhs - rhs) / abs(lhs))
+    print(f"image-leaf dot-product test: mean rel {np.mean(errs):.2e}  max {np.max(errs):.2e}")
+    assert np.mean(errs) < 1e-6 and np.max(errs) < 1e-5
+
+
+def test_image_leaf_gradient_is_adjoint_of_grid_gradient():
+    """dL/dimage = Re(A^H dL/dgrids): the image gradient of L = 1/2 sum w |V - P|^2 through the
+    facet machine equals the oracle adjoint applied to the grid gradients (1e-5 relative RMS), and
+    the Jones gradient is the same whether the grids or the image are the leaf."""
+    from oracle import facets as OF
+    from ddfacet_b200.autograd import model_grids, predict, setup_from_facet_machine
+
+    fm, vs, jd = _image_problem("regular")
+    setup = setup_from_facet_machine(fm, vs, jd)
+    rng = np.random.default_rng(9)
+    img = np.zeros((fm.nband, fm.npol, fm.npix_out, fm.npix_out), np.float32)
+    img[0, 0, rng.integers(0, fm.npix_out, 20), rng.integers(0, fm.npix_out, 20)] = rng.uniform(0.1, 1.0, 20)
+    V = torch.from_numpy((rng.standard_normal(vs.vis.shape) + 1j * rng.standard_normal(vs.vis.shape))
+                         .astype(np.complex64)).cuda() * 0.01
+    w = vs.weights
+
+    def loss_of(P):
+        r = V - P
+        return 0.5 * torch.sum(w[:, :, None] * (r.real ** 2 + r.imag ** 2))
+
+    x = torch.from_numpy(img).cuda().requires_grad_(True)
+    k1 = jd.kms.clone().requires_grad_(True)
+    loss_of(predict(setup, model_grids(fm, x), k1)).backward()
+    grids = [g.detach().requires_grad_(True) for g in model_grids(fm, torch.from_numpy(img).cuda())]
+    k2 = jd.kms.clone().requires_grad_(True)
+    loss_of(predict(setup, grids, k2)).backward()
+    want = np.zeros(img.shape, np.float64)
+    for f, g in zip(fm.facets, grids):
+        want += OF.give_model_tessel_adjoint(g.grad.cpu().numpy(), fm.facet_norm_host, f.sphe.cpu().numpy(), f.sw_host,
+                                             *f.geom.pix_central, fm.npix_out, fm.overs)
+    e = cases.rel_rms(x.grad.cpu().numpy(), want)
+    print(f"image gradient vs oracle adjoint of the grid gradients: {e:.2e}")
+    assert e < 1e-5
+    assert cases.rel_rms(k1.grad.cpu().numpy(), k2.grad.cpu().numpy()) < 1e-6
+
+
+def test_model_grids_checks_shape():
+    from ddfacet_b200.autograd import model_grids
+
+    fm, _, _ = _image_problem("regular")
+    with pytest.raises(ValueError, match="model image must be"):
+        model_grids(fm, torch.zeros((1, 1, 10, 10), device="cuda"))
+    with pytest.raises(ValueError, match="real"):
+        model_grids(fm, torch.zeros((1, 1, fm.npix_out, fm.npix_out), dtype=torch.complex64, device="cuda"))
