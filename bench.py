@@ -365,6 +365,38 @@ def run_gpu(args):
                 "what": "mode-1 map, GridDecorr 0.02, l = image radius x sqrt 2, wall time incl. host grouping"}
     del bmap
 
+    # Differentiation (the prediction as a torch.autograd.Function, ddfacet_b200.autograd): the
+    # forward prediction, then the backward passes for every facet's model grid (adjoint gridding
+    # kernel) and the per-facet per-antenna Jones, timed on the device.
+    diff_info = None
+    if w.jones is not None:
+        from ddfacet_b200.autograd import PredictSetup, predict
+        setup = PredictSetup(vs=w.vs, facets=w.facets_model, pol=w.pol, jones=w.jones)
+        leaves = [f.grid.detach().clone().requires_grad_(True) for f in w.facets_model]
+        kms_leaf = w.jones.kms.detach().clone().requires_grad_(True)
+
+        def diff_pass(ev=None):
+            if ev:
+                ev[0].record(stream)
+            P = predict(setup, leaves, kms_leaf)
+            if ev:
+                ev[1].record(stream)
+            grads = torch.autograd.grad(P, [*leaves, kms_leaf], grad_outputs=w.vs.vis)
+            if ev:
+                ev[2].record(stream)
+            return grads
+
+        diff_pass()
+        torch.cuda.synchronize()
+        de = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+        grads = diff_pass(de)
+        torch.cuda.synchronize()
+        fwd_ms, bwd_ms = de[0].elapsed_time(de[1]), de[1].elapsed_time(de[2])
+        del grads, leaves, kms_leaf
+        diff_info = {"forward_ms": round(fwd_ms, 1), "backward_ms": round(bwd_ms, 1),
+                     "Mvis_per_s": round(w.nvis / ((fwd_ms + bwd_ms) * 1e-3) / 1e6, 2),
+                     "what": "predict (all facets) + backward for all model grids and the kMS Jones"}
+
     plain_ms = None
     if args.plain:
         plain_step()
@@ -432,6 +464,7 @@ def run_gpu(args):
                    "batched_speedup": round(plain_ms / ms_step, 2)}),
         "facets_per_launch": fpl,
         "bda_map": bda_info,
+        "differentiation": diff_info,
         "imaging_weights": dict(weights_info, frac_of_hbm=round(weights_info["achieved_GBs"] / _peaks()[0], 4)),
         "roofline": {
             "bound": "hbm", "kernel": dom, "achieved": round(achieved, 2), "peak": hbm_peak, "unit": "GB/s",

@@ -303,6 +303,8 @@ extern "C" int ddfg_degrid_jones_grad(const ddfg_vis *vs, const ddfg_jones *js, 
                           "degrid_jones_grad: needs kMS Jones only, nearest direction, no amplitude/phase "
                           "normalisation");
   if (!grad_kms) return ddfg_set_error(DDFG_EINVAL, "degrid_jones_grad: null gradient array");
+  if ((uintptr_t)grad_kms & 15)
+    return ddfg_set_error(DDFG_EINVAL, "degrid_jones_grad: the gradient array must be 16-byte aligned");
   if (nfacets == 0 || vs->nblocks == 0) return DDFG_OK;
   return ddfg_launch_jones_grad(vs, js, facets, nfacets, policy, pol->npol, grad_kms, ddfg_num_ctas(4),
                                 (cudaStream_t)stream);

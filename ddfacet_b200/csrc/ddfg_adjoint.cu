@@ -201,6 +201,76 @@ __global__ void __launch_bounds__(256) degrid_adjoint_kernel(const ddfg_vis vs, 
   }
 }
 
+__device__ __forceinline__ size_t kms_offset(const ddfg_jones &js, int t, int dir, int a, int c) {
+  const size_t nd = (size_t)js.kms_dims[1], na = (size_t)js.kms_dims[2], nch = (size_t)js.kms_dims[3];
+  return (((size_t)t * nd + (size_t)dir) * na + (size_t)a) * nch * 4 + (size_t)c * 4;
+}
+
+__device__ __forceinline__ M2 load_m2(const float2 *J, size_t o) {
+  M2 m;
+#pragma unroll
+  for (int p = 0; p < 4; ++p) m.v[p] = J[o + p];
+  return m;
+}
+
+__device__ __forceinline__ M2 m2_zero() {
+  M2 m;
+#pragma unroll
+  for (int p = 0; p < 4; ++p) m.v[p] = czero();
+  return m;
+}
+
+__device__ __forceinline__ M2 m2_add(const M2 &a, const M2 &b) {
+  M2 m;
+#pragma unroll
+  for (int p = 0; p < 4; ++p) m.v[p] = cadd(a.v[p], b.v[p]);
+  return m;
+}
+
+// One 2x2 gradient cell (32-byte aligned: Jones cells are 4 complex64) += d, two vector reductions.
+__device__ __forceinline__ void red_add_m2(float2 *p, const M2 &d) {
+  asm volatile("red.global.add.v4.f32 [%0], {%1, %2, %3, %4};" ::"l"(p), "f"(d.v[0].x), "f"(d.v[0].y),
+               "f"(d.v[1].x), "f"(d.v[1].y) : "memory");
+  asm volatile("red.global.add.v4.f32 [%0], {%1, %2, %3, %4};" ::"l"(p + 2), "f"(d.v[2].x), "f"(d.v[2].y),
+               "f"(d.v[3].x), "f"(d.v[3].y) : "memory");
+}
+
+// grad[o0] += d0 and grad[o1] += d1 for every active lane; called by the whole warp.  When every
+// active lane targets the same two cells (a row's channels, a baseline's consecutive blocks in
+// one Jones slot) the warp sums first and one lane adds, instead of 32 lanes adding to the same
+// addresses.
+__device__ __forceinline__ void warp_add_jones_grad(float2 *grad, bool active, size_t o0, size_t o1, M2 d0, M2 d1,
+                                                    int lane) {
+  const unsigned act = __ballot_sync(0xffffffffu, active);
+  if (!act) return;
+  const int first = __ffs(act) - 1;
+  const unsigned long long f0 = __shfl_sync(0xffffffffu, (unsigned long long)o0, first);
+  const unsigned long long f1 = __shfl_sync(0xffffffffu, (unsigned long long)o1, first);
+  if (__all_sync(0xffffffffu, !active || ((unsigned long long)o0 == f0 && (unsigned long long)o1 == f1))) {
+    if (!active) {
+      d0 = m2_zero();
+      d1 = m2_zero();
+    }
+#pragma unroll
+    for (int p = 0; p < 4; ++p) {
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) {
+        d0.v[p].x += __shfl_xor_sync(0xffffffffu, d0.v[p].x, off);
+        d0.v[p].y += __shfl_xor_sync(0xffffffffu, d0.v[p].y, off);
+        d1.v[p].x += __shfl_xor_sync(0xffffffffu, d1.v[p].x, off);
+        d1.v[p].y += __shfl_xor_sync(0xffffffffu, d1.v[p].y, off);
+      }
+    }
+    if (lane == first) {
+      red_add_m2(grad + f0, d0);
+      red_add_m2(grad + f1, d1);
+    }
+  } else if (active) {
+    red_add_m2(grad + o0, d0);
+    red_add_m2(grad + o1, d1);
+  }
+}
+
 // dLoss/dJ_kMS* for every visibility and facet: the forward gather of the model grid, then the
 // two antenna terms, reduced into the gradient array (same layout as the Jones array).
 template <int NPOL, int SLOTS>
@@ -224,7 +294,6 @@ __global__ void __launch_bounds__(256) jones_grad_kernel(const ddfg_vis vs, cons
   float2 *wpart = partial + warp * 32 * 32;
   LaneTaps<SLOTS> lt;
   lt.reset();
-  const size_t na = (size_t)js.kms_dims[2], nch = (size_t)js.kms_dims[3], nd = (size_t)js.kms_dims[1];
   const float2 *J = (const float2 *)js.kms;
   for (int64_t s = (int64_t)blockIdx.x * nwarps + warp; s < nstripes; s += (int64_t)gridDim.x * nwarps) {
     const int64_t b = s * 32 + lane;
@@ -242,47 +311,26 @@ __global__ void __launch_bounds__(256) jones_grad_kernel(const ddfg_vis vs, cons
       if (valid) job = tap_job(geo, in.gridchan, f);
       float2 mine[NPOL];
       gather_records<NPOL, SLOTS>(valid, job, f, lt, wpart, lane, mine);
+      size_t o0 = 0, o1 = 0;
+      M2 d0 = m2_zero(), d1 = m2_zero();
       if (valid) {
-      float2 sv[4];
+        float2 sv[4];
 #pragma unroll
-      for (int p = 0; p < 4; ++p) sv[p] = (p < NPOL) ? mine[p] : czero();
-      const M2 m = corr_from_stokes(policy, sv);
-      const size_t o0 = (((size_t)in.jx.tk * nd + (size_t)f.idir_kms) * na + (size_t)in.jx.a0) * nch * 4 +
-                        (size_t)in.jx.ck * 4;
-      const size_t o1 = (((size_t)in.jx.tk * nd + (size_t)f.idir_kms) * na + (size_t)in.jx.a1) * nch * 4 +
-                        (size_t)in.jx.ck * 4;
-      M2 j0, j1;
-#pragma unroll
-      for (int p = 0; p < 4; ++p) {
-        j0.v[p] = J[o0 + p];
-        j1.v[p] = J[o1 + p];
+        for (int p = 0; p < 4; ++p) sv[p] = (p < NPOL) ? mine[p] : czero();
+        const M2 m = corr_from_stokes(policy, sv);
+        o0 = kms_offset(js, in.jx.tk, f.idir_kms, in.jx.a0, in.jx.ck);
+        o1 = kms_offset(js, in.jx.tk, f.idir_kms, in.jx.a1, in.jx.ck);
+        const M2 j0 = load_m2(J, o0), j1 = load_m2(J, o1);
+        const float dec = (float)decorr_factor(vs, f, in.nu, in.irow);
+        const float2 ph = cscale(phasor_turns(in.nu * (in.U * f.l0 + in.V * f.m0 + in.W * s_n0m1[fi]) * kInvC), dec);
+        const M2 q = m2_scale(m2_times(m, m2_herm(j1)), ph);  // d ph L(s) J1^H
+        const M2 r = m2_scale(m2_times(j0, m), ph);           // d ph J0 L(s)
+        d0 = m2_times(g, m2_herm(q));
+        d1 = m2_times(m2_herm(g), r);
       }
-      const float dec = (float)decorr_factor(vs, f, in.nu, in.irow);
-      const float2 ph = cscale(phasor_turns(in.nu * (in.U * f.l0 + in.V * f.m0 + in.W * s_n0m1[fi]) * kInvC), dec);
-      const M2 q = m2_scale(m2_times(m, m2_herm(j1)), ph);  // d ph L(s) J1^H
-      const M2 r = m2_scale(m2_times(j0, m), ph);           // d ph J0 L(s)
-      const M2 d0 = m2_times(g, m2_herm(q));
-      const M2 d1 = m2_times(m2_herm(g), r);
-#pragma unroll
-      for (int p = 0; p < 4; ++p) {
-        red_add(grad + o0 + p, d0.v[p]);
-        red_add(grad + o1 + p, d1.v[p]);
-      }
-      }
+      warp_add_jones_grad(grad, valid, o0, o1, d0, d1, lane);
     }
   }
-}
-
-__device__ __forceinline__ size_t kms_offset(const ddfg_jones &js, int t, int dir, int a, int c) {
-  const size_t nd = (size_t)js.kms_dims[1], na = (size_t)js.kms_dims[2], nch = (size_t)js.kms_dims[3];
-  return (((size_t)t * nd + (size_t)dir) * na + (size_t)a) * nch * 4 + (size_t)c * 4;
-}
-
-__device__ __forceinline__ M2 load_m2(const float2 *J, size_t o) {
-  M2 m;
-#pragma unroll
-  for (int p = 0; p < 4; ++p) m.v[p] = J[o + p];
-  return m;
 }
 
 // dLoss/dJ_kMS* for averaged blocks: the block's model sample M = L(s) is gathered once per facet;
@@ -324,57 +372,60 @@ __global__ void __launch_bounds__(256) jones_grad_block_kernel(const ddfg_vis vs
       if (valid) job = tap_job(geo, d.gridchan, f);
       float2 mine[NPOL];
       gather_records<NPOL, SLOTS>(valid, job, f, lt, wpart, lane, mine);
-      if (!valid) continue;
-      float2 sv[4];
+      // the lane's pending sums for one pair of Jones cells (o0, o1): visibilities of a row share
+      // them, so the lane adds once per run and the warp combines the last runs
+      size_t o0 = 0, o1 = 0;
+      M2 d0 = m2_zero(), d1 = m2_zero();
+      bool pending = false;
+      if (valid) {
+        float2 sv[4];
 #pragma unroll
-      for (int p = 0; p < 4; ++p) sv[p] = (p < NPOL) ? mine[p] : czero();
-      const M2 m = corr_from_stokes(policy, sv);
-      const int mid = d.rows[d.nrows / 2];
-      const float dec = (float)decorr_factor(vs, f, d.freqmean, mid);
-      M2 G;
-#pragma unroll
-      for (int p = 0; p < 4; ++p) G.v[p] = czero();
-      for (int inx = 0; inx < d.nrows; ++inx) {
-        const int64_t irow = d.rows[inx];
-        const double *up = vs.uvw + 3 * irow;
-        const double dot = up[0] * f.l0 + up[1] * f.m0 + up[2] * s_n0m1[fi];
-        for (int ch = d.ch0; ch < d.ch1; ++ch) {
-          const float2 ph = cscale(phasor_turns(vs.freqs[ch] * dot * kInvC), dec);
-          const M2 g = load_corr_matrix(vs, irow, ch);
-          if (js.mode == 1) {
-            const JonesIdx x = jones_idx(js, irow, ch);
-            const size_t o0 = kms_offset(js, x.tk, f.idir_kms, x.a0, x.ck);
-            const size_t o1 = kms_offset(js, x.tk, f.idir_kms, x.a1, x.ck);
-            const M2 j0 = load_m2(J, o0), j1 = load_m2(J, o1);
-            const M2 q = m2_scale(m2_times(m, m2_herm(j1)), ph);  // d ph L(s) J1^H
-            const M2 r = m2_scale(m2_times(j0, m), ph);           // d ph J0 L(s)
-            const M2 d0 = m2_times(g, m2_herm(q));
-            const M2 d1 = m2_times(m2_herm(g), r);
-#pragma unroll
-            for (int p = 0; p < 4; ++p) {
-              red_add(grad + o0 + p, d0.v[p]);
-              red_add(grad + o1 + p, d1.v[p]);
+        for (int p = 0; p < 4; ++p) sv[p] = (p < NPOL) ? mine[p] : czero();
+        const M2 m = corr_from_stokes(policy, sv);
+        const int mid = d.rows[d.nrows / 2];
+        const float dec = (float)decorr_factor(vs, f, d.freqmean, mid);
+        M2 G = m2_zero();
+        for (int inx = 0; inx < d.nrows; ++inx) {
+          const int64_t irow = d.rows[inx];
+          const double *up = vs.uvw + 3 * irow;
+          const double dot = up[0] * f.l0 + up[1] * f.m0 + up[2] * s_n0m1[fi];
+          for (int ch = d.ch0; ch < d.ch1; ++ch) {
+            const float2 ph = cscale(phasor_turns(vs.freqs[ch] * dot * kInvC), dec);
+            const M2 g = load_corr_matrix(vs, irow, ch);
+            if (js.mode == 1) {
+              const JonesIdx x = jones_idx(js, irow, ch);
+              const size_t p0 = kms_offset(js, x.tk, f.idir_kms, x.a0, x.ck);
+              const size_t p1 = kms_offset(js, x.tk, f.idir_kms, x.a1, x.ck);
+              if (pending && (p0 != o0 || p1 != o1)) {
+                red_add_m2(grad + o0, d0);
+                red_add_m2(grad + o1, d1);
+                d0 = m2_zero();
+                d1 = m2_zero();
+              }
+              o0 = p0;
+              o1 = p1;
+              pending = true;
+              const M2 j0 = load_m2(J, p0), j1 = load_m2(J, p1);
+              const M2 q = m2_scale(m2_times(m, m2_herm(j1)), ph);  // d ph L(s) J1^H
+              const M2 r = m2_scale(m2_times(j0, m), ph);           // d ph J0 L(s)
+              d0 = m2_add(d0, m2_times(g, m2_herm(q)));
+              d1 = m2_add(d1, m2_times(m2_herm(g), r));
+            } else {
+              G = m2_add(G, m2_scale(g, cconj(ph)));
             }
-          } else {
-            const M2 gp = m2_scale(g, cconj(ph));
-#pragma unroll
-            for (int p = 0; p < 4; ++p) G.v[p] = cadd(G.v[p], gp.v[p]);
           }
         }
-      }
-      if (js.mode == 2) {
-        const JonesIdx x = jones_idx(js, mid, (d.ch0 + d.ch1) / 2);
-        const size_t o0 = kms_offset(js, x.tk, f.idir_kms, x.a0, x.ck);
-        const size_t o1 = kms_offset(js, x.tk, f.idir_kms, x.a1, x.ck);
-        const M2 j0 = load_m2(J, o0), j1 = load_m2(J, o1);
-        const M2 d0 = m2_times(G, m2_herm(m2_times(m, m2_herm(j1))));
-        const M2 d1 = m2_times(m2_herm(G), m2_times(j0, m));
-#pragma unroll
-        for (int p = 0; p < 4; ++p) {
-          red_add(grad + o0 + p, d0.v[p]);
-          red_add(grad + o1 + p, d1.v[p]);
+        if (js.mode == 2) {
+          const JonesIdx x = jones_idx(js, mid, (d.ch0 + d.ch1) / 2);
+          o0 = kms_offset(js, x.tk, f.idir_kms, x.a0, x.ck);
+          o1 = kms_offset(js, x.tk, f.idir_kms, x.a1, x.ck);
+          const M2 j0 = load_m2(J, o0), j1 = load_m2(J, o1);
+          d0 = m2_times(G, m2_herm(m2_times(m, m2_herm(j1))));
+          d1 = m2_times(m2_herm(G), m2_times(j0, m));
+          pending = true;
         }
       }
+      warp_add_jones_grad(grad, pending, o0, o1, d0, d1, lane);
     }
   }
 }

@@ -178,7 +178,7 @@ int ddfg_degrid_adjoint(const ddfg_vis *vs, const ddfg_jones *js, const ddfg_pol
 
 /* Backward pass of ddfg_degrid for the kMS Jones terms: with vs->vis = dLoss/dP* as above and
  * facets[i].grid the model grids of the forward pass, adds dLoss/dJ* to grad_kms (complex64,
- * the layout of js->kms, +=).  Needs kMS Jones only, nearest direction, no amplitude/phase
+ * the layout of js->kms, 16-byte aligned, +=).  Needs kMS Jones only, nearest direction, no amplitude/phase
  * normalisation (DDFG_EUNSUPPORTED otherwise); any BDA map, per-visibility or per-block
  * (BDAJones) Jones.  No counterpart in the reference. */
 int ddfg_degrid_jones_grad(const ddfg_vis *vs, const ddfg_jones *js, const ddfg_pol *pol,

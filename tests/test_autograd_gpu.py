@@ -114,9 +114,9 @@ def test_finite_differences_fp64(kind, jones_mode):
     # 32 Jones coordinates (used slots, directions and antennas) and 32 model-grid coordinates
     used_t = np.unique(cs[0].jones["kms_tmap"])
     for n in range(64):
-        kind = "jones" if n < 32 else "grid"
+        coord = "jones" if n < 32 else "grid"
         imag = bool(rng.integers(2))
-        if kind == "jones":
+        if coord == "jones":
             idx = (int(rng.choice(used_t)), int(rng.integers(1, 3)), int(rng.integers(0, cs[0].obs.nant)), 0,
                    int(rng.integers(2)), int(rng.integers(2)))
             base = kms
@@ -131,7 +131,7 @@ def test_finite_differences_fp64(kind, jones_mode):
         plus, minus = base.copy(), base.copy()
         plus[idx] += np.complex64(step)
         minus[idx] -= np.complex64(step)
-        if kind == "jones":
+        if coord == "jones":
             lp = _oracle_loss(cs, grids, plus, V, w)
             lm = _oracle_loss(cs, grids, minus, V, w)
         else:
@@ -239,9 +239,11 @@ def test_image_to_grid_adjoint_matches_oracle(kind):
 
 
 def test_image_leaf_dot_product_256_pairs():
-    """Re <y, P(x)> = <x, grad> for the whole chain real image x -> facet grids -> prediction with
+    """<y, P(x)> = <x, A^H y> for the whole chain real image x -> facet grids -> prediction with
     per-facet Jones, over 256 random pairs: relative difference <= 1e-6 in the mean, 1e-5 for any
-    pair (float64 inner products of the float32 results)."""
+    pair (float64 inner products of the float32 results).  For a real leaf the backward pass gives
+    Re(A^H y) = d Re<y, P>/dx; the imaginary part comes from a second backward pass with i y
+    (Re<i y, P> = Im<y, P>), so the complex products are compared as in the model-grid test."""
     from ddfacet_b200.autograd import model_grids, predict, setup_from_facet_machine
 
     fm, vs, jd = _image_problem("voronoi")
@@ -254,9 +256,11 @@ def test_image_leaf_dot_product_256_pairs():
         y = torch.from_numpy((rng.standard_normal(vs.vis.shape) + 1j * rng.standard_normal(vs.vis.shape))
                              .astype(np.complex64)).cuda()
         P = predict(setup, model_grids(fm, x), jd.kms)
-        (gx,) = torch.autograd.grad(P, [x], grad_outputs=y)
-        lhs = _vdot(y, P.detach()).real
-        rhs = float(torch.sum(gx.double() * x.detach().double()).item())
+        (gr,) = torch.autograd.grad(P, [x], grad_outputs=y, retain_graph=True)
+        (gi,) = torch.autograd.grad(P, [x], grad_outputs=1j * y)
+        lhs = _vdot(y, P.detach())
+        xd = x.detach().double()
+        rhs = complex(float(torch.sum(gr.double() * xd).item()), float(torch.sum(gi.double() * xd).item()))
         errs.append(abs(lhs - rhs) / abs(lhs))
     print(f"image-leaf dot-product test: mean rel {np.mean(errs):.2e}  max {np.max(errs):.2e}")
     assert np.mean(errs) < 1e-6 and np.max(errs) < 1e-5
