@@ -23,6 +23,7 @@ import itertools
 import math
 
 import numpy as np
+import torch
 
 C_BDA = 3e8
 
@@ -218,8 +219,6 @@ def smear_mapping_gpu(A0, A1, uvw, freqs, dfreq, dPhi, l, chan_map, device=None)
     """Mode-1 map (``GiveBlocksRowsListBL_old`` for every baseline, packed as
     ``collectSmearMapping`` does) built on the GPU by ddfg_bda_mode1_count / _write: the same
     words as ``smear_mapping(..., mode=1)``.  Returns an int32 device tensor."""
-    import torch
-
     from . import _abi, device as D
 
     dev = D._dev(device)
@@ -263,3 +262,55 @@ def smear_mapping_gpu(A0, A1, uvw, freqs, dfreq, dPhi, l, chan_map, device=None)
     _abi.check(lib.ddfg_bda_mode1_write(*args, blk_off.data_ptr(), word_off.data_ptr(), m[2:].data_ptr(),
                                         m[2 + nb:].data_ptr(), st))
     return m
+
+
+def _spread_bits16(x: torch.Tensor) -> torch.Tensor:
+    """Bits 0..15 of x moved to the even bit positions 0..30."""
+    x = (x | (x << 8)) & 0x00FF00FF
+    x = (x | (x << 4)) & 0x0F0F0F0F
+    x = (x | (x << 2)) & 0x33333333
+    return (x | (x << 1)) & 0x55555555
+
+
+def uv_locality_order(bda_map: torch.Tensor, block_start: torch.Tensor, uvw: torch.Tensor, freqs: torch.Tensor,
+                      tile_wavelengths: float) -> torch.Tensor:
+    """A permutation of a packed map's blocks (int64 [nblocks]) that visits them in Z order of
+    uv tiles: each block's first row and first channel give (u, v) in wavelengths, cut into
+    tiles of ``tile_wavelengths``.  The same order suits every facet, whose grid positions are
+    the uv coordinates scaled by the facet's size (plus a small w shift)."""
+    nb = block_start.numel()
+    if nb == 0:
+        return torch.zeros(0, dtype=torch.int64, device=bda_map.device)
+    ch0 = bda_map[block_start].to(torch.int64)
+    row = bda_map[block_start + 2].to(torch.int64)
+    lam = freqs.to(torch.float64)[ch0] / 299792458.0
+    u = uvw[row, 0] * lam
+    v = uvw[row, 1] * lam
+    t = float(tile_wavelengths)
+    iu = torch.floor(u / t).to(torch.int64)
+    iv = torch.floor(v / t).to(torch.int64)
+    iu = (iu - iu.min()).clamp_(0, 0xFFFF)
+    iv = (iv - iv.min()).clamp_(0, 0xFFFF)
+    key = _spread_bits16(iu) | (_spread_bits16(iv) << 1)
+    return torch.sort(key, stable=True)[1]
+
+
+def reorder_blocks(bda_map: torch.Tensor, block_start: torch.Tensor, order: torch.Tensor) -> torch.Tensor:
+    """The packed map (int32, on the map's device) with its blocks in ``order`` (a permutation of
+    block indices): the same blocks, so the degridder's result is unchanged and the gridder's
+    differs only by the order of its floating-point sums."""
+    nb = block_start.numel()
+    if nb == 0:
+        return bda_map.clone()
+    sizes = bda_map[2:2 + nb].to(torch.int64)
+    s = sizes[order]
+    starts = block_start[order]
+    new_off = torch.cumsum(s, 0) - s
+    total = int(s.sum().item())
+    base = 2 + nb
+    idx = torch.repeat_interleave(starts - new_off, s) + torch.arange(total, device=bda_map.device)
+    out = torch.empty(base + total, dtype=torch.int32, device=bda_map.device)
+    out[:2] = bda_map[:2]
+    out[2:base] = s.to(torch.int32)
+    out[base:] = bda_map[idx]
+    return out
