@@ -273,11 +273,14 @@ def _spread_bits16(x: torch.Tensor) -> torch.Tensor:
 
 
 def uv_locality_order(bda_map: torch.Tensor, block_start: torch.Tensor, uvw: torch.Tensor, freqs: torch.Tensor,
-                      tile_wavelengths: float) -> torch.Tensor:
+                      tile_wavelengths: float, w_planes=None) -> torch.Tensor:
     """A permutation of a packed map's blocks (int64 [nblocks]) that visits them in Z order of
     uv tiles: each block's first row and first channel give (u, v) in wavelengths, cut into
     tiles of ``tile_wavelengths``.  The same order suits every facet, whose grid positions are
-    the uv coordinates scaled by the facet's size (plus a small w shift)."""
+    the uv coordinates scaled by the facet's size (plus a small w shift).  With ``w_planes`` =
+    (Nw, wmax), blocks of a tile are further ordered by their W plane, lrint((Nw-1) |w| nu /
+    (nu_max wmax)) (gridder.h:324 with RefWave = c / nu_max), which every facet shares: runs of
+    equal support."""
     nb = block_start.numel()
     if nb == 0:
         return torch.zeros(0, dtype=torch.int64, device=bda_map.device)
@@ -292,6 +295,11 @@ def uv_locality_order(bda_map: torch.Tensor, block_start: torch.Tensor, uvw: tor
     iu = (iu - iu.min()).clamp_(0, 0xFFFF)
     iv = (iv - iv.min()).clamp_(0, 0xFFFF)
     key = _spread_bits16(iu) | (_spread_bits16(iv) << 1)
+    if w_planes is not None:
+        nw, wmax = int(w_planes[0]), float(w_planes[1])
+        fr = freqs.to(torch.float64)
+        iw = torch.round((nw - 1) * uvw[row, 2].abs() * fr[ch0] / (fr.max() * wmax)).to(torch.int64)
+        key = (key << 8) | iw.clamp_(0, 255)
     return torch.sort(key, stable=True)[1]
 
 

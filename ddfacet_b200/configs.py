@@ -183,12 +183,13 @@ def row_chunks(w: Workload, nchunks: int) -> List[pipeline.Chunk]:
 
 
 def uneven_bda(device=None, scale=1.0, seed=1003, nfacets=25, npix_image=6000, cell=1.0, nchan=128, nw=32,
-               grid_decorr=0.02, nsrc=200):
+               grid_decorr=0.02, nsrc=200, block_order_tile=256):
     """Uneven facets with baseline-dependent averaging: a 6000^2 image at 1"/pixel in a Voronoi
     tessellation around 25 directions, 48 antennas in a 12 km log-radial layout, 6 h at 4 s,
     128 channels 0.9-1.7 GHz, 4 correlations, per-facet per-antenna 5-min Jones; block map of
     DDFacet's default mode 1 with GridDecorr 0.02 over the largest facet's field, built on the
-    GPU (every block averages a few rows and channels, more on short baselines)."""
+    GPU (every block averages a few rows and channels, more on short baselines), its blocks
+    visited in uv Z order (``block_order_tile`` cells per tile; 0 keeps the map order)."""
     dev = D._dev(device)
     hours = 6.0 * scale
     obs = synth.make_observation(seed, 48, 12000.0, 34.0, 40.0, hours, 4.0, nchan, 0.90e9, 1.70e9, layout="lograd")
@@ -211,6 +212,13 @@ def uneven_bda(device=None, scale=1.0, seed=1003, nfacets=25, npix_image=6000, c
     bmap = bda.smear_mapping_gpu(obs.A0, obs.A1, uvw_d, obs.freqs, dfreq, np.sqrt(6 * grid_decorr), lmax, chan_map,
                                  device=dev)
     vs = D.VisData.create(vis, uvw_d, flags, weights, obs.freqs, chan_map, bmap, device=dev)
+    if block_order_tile:
+        # blocks in Z order of uv tiles of `block_order_tile` cells of the largest facet's grid:
+        # the blocks in flight at once share a small piece of every facet's grid (L2-resident)
+        # while a stripe of 32 blocks stays on one baseline
+        tile = block_order_tile / (max(f.npix_padded for f in tess.facets) * tess.cell_rad)
+        vs = vs.with_block_order(bda.uv_locality_order(vs.bda_map, vs.block_start, vs.uvw, vs.freqs, tile))
+        del bmap
     nt = int(np.ceil(hours * 3600 / 300.0))
     J = synth.random_jones(seed + 3, nt, nfacets, 48, 1, 0.1)
     tmap = np.minimum(((obs.times - obs.times.min()) // 300.0).astype(np.int32), nt - 1)
@@ -236,6 +244,7 @@ def uneven_bda(device=None, scale=1.0, seed=1003, nfacets=25, npix_image=6000, c
     w = Workload("uneven_bda", vs, fg, fm, jd, pol, nvis=nrow * nchan, nrow=nrow, nchan=nchan, ncorr=ncorr,
                  nfacets=len(fg))
     w.info = dict(npix=tess.npix, grids=[f.npix_padded for f in tess.facets], nw=nw, nblocks=vs.nblocks,
+                  block_order=(f"uv Z order, tiles of {block_order_tile} cells" if block_order_tile else "map order"),
                   vis_per_block=nrow * nchan / max(vs.nblocks, 1), wmax=wmax, nant=48, ntimes=obs.ntimes)
     w.host = {"obs": obs, "wterms": wts, "tess": tess, "chan_map": chan_map}
     return w

@@ -15,7 +15,7 @@ PyTorch tensors own all device memory (plumbing only); the work is done by libdd
 from __future__ import annotations
 
 import ctypes as C
-from dataclasses import dataclass, field
+from dataclasses import dataclass, field, replace
 from typing import List, Optional, Sequence
 
 import numpy as np
@@ -147,6 +147,19 @@ class VisData:
             out.uvw_dt = to_device(uvw_dt, torch.float64, device)
             out.dt, out.dnu, out.do_tsmear, out.do_fsmear = float(dt), float(dnu), int(do_t), int(do_f)
         return out
+
+    def with_block_order(self, order: torch.Tensor) -> "VisData":
+        """The same visibilities with the map's blocks visited in ``order`` (a permutation of block
+        indices, e.g. ``bda.uv_locality_order``): the map is rewritten by ``bda.reorder_blocks``
+        and planned again, and a sparsification mask is permuted with the blocks.  The degridder's
+        output changes only by the order of its tap sums, the gridder's by the order of its grid
+        sums."""
+        from . import bda
+
+        m = bda.reorder_blocks(self.bda_map, self.block_start, order)
+        starts, single = self.plan_map(m, int(self.vis.shape[0]), int(self.vis.shape[1]))
+        sp = None if self.sparsification is None else self.sparsification[order].contiguous()
+        return replace(self, bda_map=m, block_start=starts, single_vis_blocks=single, sparsification=sp)
 
     def struct(self) -> _abi.VisSet:
         s = _abi.VisSet()

@@ -101,6 +101,39 @@ def test_flags_and_sparsification():
     np.testing.assert_allclose(fg.sumwt.cpu().numpy(), r["sumwt"], rtol=1e-9)
 
 
+@pytest.mark.parametrize("jmode", [0, 1, 2])
+def test_bda_blocks_in_uv_order(jmode):
+    """The blocks of a mode-1 map visited in uv Z order (VisData.with_block_order): grid, weight
+    sums and prediction against the reference run on the original map, with a sparsification
+    mask that follows its blocks."""
+    import torch
+
+    from ddfacet_b200 import bda, device as D
+
+    c = cases.make_case(bda_mode=1, dphi=np.sqrt(6 * 0.05), nchan=16, flag_frac=0.1, ncorr=4)
+    if jmode:
+        cases.add_jones(c, mode=jmode, nt=3, nd=3)
+    nb = int(c.bda[0])
+    sp = np.random.default_rng(1).uniform(size=nb) < 0.7
+    r = cases.run_ref_grid(c, sparsification=sp)
+    model = r["grid"]
+    vr = cases.run_ref_degrid(c, model, vis0=c.vis)
+    pol = D.make_pol(c.corr_ids, c.stokes_ids)
+    vs, fg, jd = cases._gpu_objs(c)
+    vs.sparsification = torch.from_numpy(sp.astype(np.uint8)).cuda()
+    order = bda.uv_locality_order(vs.bda_map, vs.block_start, vs.uvw, vs.freqs, 200.0)
+    assert not torch.equal(order, torch.arange(nb, device=order.device))
+    vs2 = vs.with_block_order(order)
+    D.grid(vs2, [fg], pol, jd)
+    assert cases.rel_rms(fg.grid.cpu().numpy(), r["grid"]) < TOL
+    np.testing.assert_array_equal(fg.grid.cpu().numpy() != 0, r["grid"] != 0)
+    np.testing.assert_allclose(fg.sumwt.cpu().numpy(), r["sumwt"], rtol=1e-9)
+    vs2.sparsification = None
+    fm = cases._gpu_objs(c, model_grid=model)[1]
+    D.degrid(vs2, [fm], pol, jd)
+    assert cases.rel_rms(c.vis - vs2.vis.cpu().numpy(), c.vis - vr) < TOL
+
+
 @pytest.mark.parametrize("jmode,beam,kms,interp", [(1, False, True, 0), (1, True, True, 0), (2, False, True, 0),
                                                    (2, True, True, 0), (1, True, False, 0), (1, False, True, 1)])
 def test_jones(jmode, beam, kms, interp):
