@@ -153,6 +153,14 @@ __device__ __forceinline__ void norm_jones(M2 &j, const ddfg_jones &js, double u
   }
 }
 
+// Blocks of more visibilities than this are walked by the whole warp (the kernels' cooperative
+// paths) when the Jones terms do not depend on a visibility's uv (no DoScaleJones): mode-1 blocks
+// on the shortest baselines can span a whole track (10^4-10^5 visibilities), and one lane walking
+// such a block holds its warp, and the launch, for the whole walk.
+constexpr int kCoopVis = 128;
+
+__device__ __forceinline__ bool coop_blocks_ok(const ddfg_jones &js) { return js.mode == 0 || !js.scale_jones; }
+
 // Cached Jones state of one block walk.  The reference recomputes the beam and DD Jones only
 // when the antennas, the time slot or the Jones channel change; the DD Jones normalisation
 // reads the uvw of the visibility at which that happened, which is kept so the cached and

@@ -40,6 +40,7 @@ __global__ void __launch_bounds__(256) degrid_kernel(const ddfg_vis vs, const dd
   float2 *wpart = partial + warp * 32 * 32;   // [block][lane], NPOL == 1 only
   LaneTaps<SLOTS> lt;
   lt.reset();
+  const bool coop = coop_blocks_ok(js);
 
   for (int64_t s = (int64_t)blockIdx.x * nwarps + warp; s < nstripes; s += (int64_t)gridDim.x * nwarps) {
     const int64_t b = s * 32 + lane;
@@ -59,9 +60,14 @@ __global__ void __launch_bounds__(256) degrid_kernel(const ddfg_vis vs, const dd
 
       float2 mine[NPOL];
       gather_records<NPOL, SLOTS>(valid, job, f, lt, wpart, lane, mine);
-      if (valid) {
-        if (SINGLE) degrid_single_apply<NPOL>(vs, js, f, dp, sch, srow, mine);
-        else degrid_block_apply<NPOL>(vs, js, f, dp, d, mine);
+      if (SINGLE) {
+        if (valid) degrid_single_apply<NPOL>(vs, js, f, dp, sch, srow, mine);
+      } else {
+        // blocks of more than kCoopVis visibilities are applied by the whole warp
+        const bool big = valid && coop && (int64_t)d.nrows * (d.ch1 - d.ch0) > kCoopVis;
+        if (valid && !big) degrid_block_apply<NPOL>(vs, js, f, dp, d, mine);
+        for (unsigned bm = __ballot_sync(0xffffffffu, big); bm; bm &= bm - 1)
+          degrid_block_apply_warp<NPOL>(vs, js, f, dp, d, mine, __ffs(bm) - 1, lane);
       }
     }
   }

@@ -101,6 +101,26 @@ def test_flags_and_sparsification():
     np.testing.assert_allclose(fg.sumwt.cpu().numpy(), r["sumwt"], rtol=1e-9)
 
 
+@pytest.mark.parametrize("jmode,psf,scale", [(0, False, 0), (1, False, 0), (2, False, 0), (1, True, 0), (2, True, 0),
+                                             (1, False, 1)])
+def test_large_blocks(jmode, psf, scale):
+    """Mode-1 maps whose short-baseline blocks hold hundreds of visibilities, more than the
+    kernels' cooperative threshold (128; the warp walks such a block, its owner only the FP64
+    means): grid, touched cells, weight and Jones sums and prediction against the reference.
+    With DoScaleJones (uv-dependent Jones) the one-lane walk is kept."""
+    c = cases.make_case(bda_mode=1, dphi=np.sqrt(6 * 1.0), nchan=16, ntimes=60, flag_frac=0.1, ncorr=4)
+    nb = int(np.uint32(c.bda[0]))
+    sz = c.bda[2:2 + nb].astype(np.int64)
+    st = 2 + nb + np.concatenate([[0], np.cumsum(sz)[:-1]])
+    nv = (sz - 2) * (c.bda[st + 1] - c.bda[st])
+    assert (nv > 128).sum() >= 32 and nv.max() >= 900
+    if jmode:
+        cases.add_jones(c, mode=jmode, nt=3, nd=3, scale=scale, calib_err=0.05 if scale else 0.0)
+    _cmp_grid(c, dopsf=psf)
+    if not psf:
+        _cmp_degrid(c)
+
+
 @pytest.mark.parametrize("jmode", [0, 1, 2])
 def test_bda_blocks_in_uv_order(jmode):
     """The blocks of a mode-1 map visited in uv Z order (VisData.with_block_order): grid, weight
