@@ -47,6 +47,8 @@ __global__ void __launch_bounds__(256) degrid_kernel(const ddfg_vis vs, const dd
     const bool inrange = b < vs.nblocks;
     DegridBlock d;
     if (inrange && !SINGLE) degrid_block_header(vs, b, d);
+    int64_t coop_t = INT64_MAX;
+    if (!SINGLE && coop) coop_t = coop_threshold(inrange ? (int64_t)d.nrows * (d.ch1 - d.ch0) : 0, 0);
     for (int fi = 0; fi < pack.n; ++fi) {
       const ddfg_facet &f = sf[fi];
       BlockGeom g;
@@ -63,8 +65,8 @@ __global__ void __launch_bounds__(256) degrid_kernel(const ddfg_vis vs, const dd
       if (SINGLE) {
         if (valid) degrid_single_apply<NPOL>(vs, js, f, dp, sch, srow, mine);
       } else {
-        // blocks of more than kCoopVis visibilities are applied by the whole warp
-        const bool big = valid && coop && (int64_t)d.nrows * (d.ch1 - d.ch0) > kCoopVis;
+        // large blocks are applied by the whole warp (coop_threshold)
+        const bool big = valid && (int64_t)d.nrows * (d.ch1 - d.ch0) > coop_t;
         if (valid && !big) degrid_block_apply<NPOL>(vs, js, f, dp, d, mine);
         for (unsigned bm = __ballot_sync(0xffffffffu, big); bm; bm &= bm - 1)
           degrid_block_apply_warp<NPOL>(vs, js, f, dp, d, mine, __ffs(bm) - 1, lane);

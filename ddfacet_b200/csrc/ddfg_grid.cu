@@ -113,6 +113,10 @@ __global__ void __launch_bounds__(128, 3) grid_block_fi_kernel(const ddfg_vis vs
   const bool coop = coop_blocks_ok(js);
   for (int64_t s = (int64_t)blockIdx.x * nwarps + warp; s < nstripes; s += (int64_t)gridDim.x * nwarps) {
     const int64_t b = s * 32 + lane;
+    // blocks walked by the whole warp in this stripe (the same for every facet); an owner walks
+    // its block's FP64 means alone, about an eighth of the one-lane walk
+    const int64_t nvb = (b < vs.nblocks && coop) ? block_nvis(vs, b) : 0;
+    const int64_t coop_t = coop ? coop_threshold(nvb, 8) : INT64_MAX;
     for (int fi = 0; fi < pack.n; ++fi) {
       const ddfg_facet &f = sf[fi];
       const int npol_used = min(gp.nvispol, f.npol);
@@ -120,10 +124,9 @@ __global__ void __launch_bounds__(128, 3) grid_block_fi_kernel(const ddfg_vis vs
       double *a_chan = a + f.nband * f.npol + 2 * f.nband;
       GridRecord<NPOL> rec;
       rec.valid = false;
-      // blocks of more than kCoopVis visibilities: the owner walks only the FP64 means, the warp
-      // does the rest (grid_block_record_warp)
-      const bool big = b < vs.nblocks && coop && block_nvis(vs, b) > kCoopVis &&
-                       !(vs.sparsification && !vs.sparsification[b]);
+      // large blocks: the owner walks only the FP64 means, the warp does the rest
+      // (grid_block_record_warp)
+      const bool big = nvb > coop_t && !(vs.sparsification && !vs.sparsification[b]);
       BlockMeans bmeans{};
       if (big) bmeans = grid_block_means(vs, f, b);
       else if (b < vs.nblocks) grid_block_record<NPOL>(vs, js, f, gp, b, s_n0m1[fi], rec, jc);
