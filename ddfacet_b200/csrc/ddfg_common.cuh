@@ -153,49 +153,6 @@ __device__ __forceinline__ void norm_jones(M2 &j, const ddfg_jones &js, double u
   }
 }
 
-// Mode-1 blocks on the shortest baselines can span a whole track (10^4-10^5 visibilities), and one
-// lane walking such a block holds its warp, and the launch, for the whole walk.  The kernels'
-// cooperative paths walk large blocks with the whole warp when the Jones terms do not depend on
-// a visibility's uv (no DoScaleJones); coop_threshold picks which, never a block of kCoopVis
-// visibilities or fewer.
-constexpr int kCoopVis = 128;
-
-__device__ __forceinline__ bool coop_blocks_ok(const ddfg_jones &js) { return js.mode == 0 || !js.scale_jones; }
-
-// The size above which a stripe's blocks are walked cooperatively, chosen per stripe from its 32
-// block sizes nv (visibilities; 0 for a lane without a block) by comparing estimated costs in
-// serial visibility steps: one lane per block costs the largest block; walking the blocks above
-// T with the whole warp costs, for each, nv / 32 steps plus a fixed overhead, plus owner_div^-1
-// of the largest such block for work its owner does alone (0: none), plus the largest block left
-// to the lanes.  Candidates T = max / 2^j down to kCoopVis; returns INT64_MAX for no cooperative
-// walk.  All 32 lanes call it.
-__device__ __forceinline__ int64_t coop_threshold(int64_t nv, int owner_div) {
-  int64_t mx = nv;
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, o));
-  int64_t best_t = INT64_MAX, best_cost = mx;
-  for (int j = 1; j <= 8; ++j) {
-    const int64_t t = mx >> j;
-    if (t < kCoopVis) break;
-    const bool big = nv > t;
-    int64_t sum_big = big ? nv / 32 + 24 : 0;
-    int64_t max_small = big ? 0 : nv;
-    int64_t max_own = (big && owner_div > 0) ? nv / owner_div : 0;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-      sum_big += __shfl_xor_sync(0xffffffffu, sum_big, o);
-      max_small = max(max_small, __shfl_xor_sync(0xffffffffu, max_small, o));
-      max_own = max(max_own, __shfl_xor_sync(0xffffffffu, max_own, o));
-    }
-    const int64_t cost = sum_big + max_own + max_small;
-    if (cost < best_cost) {
-      best_cost = cost;
-      best_t = t;
-    }
-  }
-  return best_t;
-}
-
 // Cached Jones state of one block walk.  The reference recomputes the beam and DD Jones only
 // when the antennas, the time slot or the Jones channel change; the DD Jones normalisation
 // reads the uvw of the visibility at which that happened, which is kept so the cached and

@@ -40,15 +40,12 @@ __global__ void __launch_bounds__(256) degrid_kernel(const ddfg_vis vs, const dd
   float2 *wpart = partial + warp * 32 * 32;   // [block][lane], NPOL == 1 only
   LaneTaps<SLOTS> lt;
   lt.reset();
-  const bool coop = coop_blocks_ok(js);
 
   for (int64_t s = (int64_t)blockIdx.x * nwarps + warp; s < nstripes; s += (int64_t)gridDim.x * nwarps) {
     const int64_t b = s * 32 + lane;
     const bool inrange = b < vs.nblocks;
     DegridBlock d;
     if (inrange && !SINGLE) degrid_block_header(vs, b, d);
-    int64_t coop_t = INT64_MAX;
-    if (!SINGLE && coop) coop_t = coop_threshold(inrange ? (int64_t)d.nrows * (d.ch1 - d.ch0) : 0, 0);
     for (int fi = 0; fi < pack.n; ++fi) {
       const ddfg_facet &f = sf[fi];
       BlockGeom g;
@@ -62,14 +59,9 @@ __global__ void __launch_bounds__(256) degrid_kernel(const ddfg_vis vs, const dd
 
       float2 mine[NPOL];
       gather_records<NPOL, SLOTS>(valid, job, f, lt, wpart, lane, mine);
-      if (SINGLE) {
-        if (valid) degrid_single_apply<NPOL>(vs, js, f, dp, sch, srow, mine);
-      } else {
-        // large blocks are applied by the whole warp (coop_threshold)
-        const bool big = valid && (int64_t)d.nrows * (d.ch1 - d.ch0) > coop_t;
-        if (valid && !big) degrid_block_apply<NPOL>(vs, js, f, dp, d, mine);
-        for (unsigned bm = __ballot_sync(0xffffffffu, big); bm; bm &= bm - 1)
-          degrid_block_apply_warp<NPOL>(vs, js, f, dp, d, mine, __ffs(bm) - 1, lane);
+      if (valid) {
+        if (SINGLE) degrid_single_apply<NPOL>(vs, js, f, dp, sch, srow, mine);
+        else degrid_block_apply<NPOL>(vs, js, f, dp, d, mine);
       }
     }
   }

@@ -110,31 +110,17 @@ __global__ void __launch_bounds__(128, 3) grid_block_fi_kernel(const ddfg_vis vs
   JonesCache jc;
   LaneTaps<SLOTS> lt;
   lt.reset();
-  const bool coop = coop_blocks_ok(js);
   for (int64_t s = (int64_t)blockIdx.x * nwarps + warp; s < nstripes; s += (int64_t)gridDim.x * nwarps) {
     const int64_t b = s * 32 + lane;
-    // blocks walked by the whole warp in this stripe (the same for every facet); an owner walks
-    // its block's FP64 means alone, about an eighth of the one-lane walk
-    const int64_t nvb = (b < vs.nblocks && coop) ? block_nvis(vs, b) : 0;
-    const int64_t coop_t = coop ? coop_threshold(nvb, 8) : INT64_MAX;
     for (int fi = 0; fi < pack.n; ++fi) {
       const ddfg_facet &f = sf[fi];
       const int npol_used = min(gp.nvispol, f.npol);
       double *a = s_acc + (size_t)fi * acc_stride;
-      double *a_chan = a + f.nband * f.npol + 2 * f.nband;
       GridRecord<NPOL> rec;
       rec.valid = false;
-      // large blocks: the owner walks only the FP64 means, the warp does the rest
-      // (grid_block_record_warp)
-      const bool big = nvb > coop_t && !(vs.sparsification && !vs.sparsification[b]);
-      BlockMeans bmeans{};
-      if (big) bmeans = grid_block_means(vs, f, b);
-      else if (b < vs.nblocks) grid_block_record<NPOL>(vs, js, f, gp, b, s_n0m1[fi], rec, jc);
-      for (unsigned bm = __ballot_sync(0xffffffffu, big); bm; bm &= bm - 1)
-        grid_block_record_warp<NPOL>(vs, js, f, gp, b, bmeans, s_n0m1[fi], __ffs(bm) - 1, lane, npol_used, a_chan,
-                                     rec);
-      warp_add_block_sums<NPOL, false>(vs, js, f, gp, b, rec, npol_used, a, a + f.nband * f.npol, a_chan, jc,
-                                       big && !rec.single_chan);
+      if (b < vs.nblocks) grid_block_record<NPOL>(vs, js, f, gp, b, s_n0m1[fi], rec, jc);
+      warp_add_block_sums<NPOL, false>(vs, js, f, gp, b, rec, npol_used, a, a + f.nband * f.npol,
+                                       a + f.nband * f.npol + 2 * f.nband, jc);
       scatter_records<NPOL, SLOTS>(rec, f, npol_used, lt, lane);
     }
   }

@@ -104,10 +104,9 @@ def test_flags_and_sparsification():
 @pytest.mark.parametrize("jmode,psf,scale", [(0, False, 0), (1, False, 0), (2, False, 0), (1, True, 0), (2, True, 0),
                                              (1, False, 1)])
 def test_large_blocks(jmode, psf, scale):
-    """Mode-1 maps whose short-baseline blocks hold hundreds of visibilities, more than the
-    kernels' cooperative threshold (128; the warp walks such a block, its owner only the FP64
-    means): grid, touched cells, weight and Jones sums and prediction against the reference.
-    With DoScaleJones (uv-dependent Jones) the one-lane walk is kept."""
+    """Mode-1 maps whose short-baseline blocks hold hundreds of visibilities (one lane walks
+    each): grid, touched cells, weight and Jones sums and prediction against the reference, with
+    per-visibility, per-block and uv-dependent (DoScaleJones) Jones and in PSF mode."""
     c = cases.make_case(bda_mode=1, dphi=np.sqrt(6 * 1.0), nchan=16, ntimes=60, flag_frac=0.1, ncorr=4)
     nb = int(np.uint32(c.bda[0]))
     sz = c.bda[2:2 + nb].astype(np.int64)
