@@ -55,6 +55,7 @@ class VisSet(C.Structure):
         ("bda_map", _vp), ("bda_len", _i64), ("block_start", _vp), ("nblocks", _i64),
         ("sparsification", _vp),
         ("uvw_dt", _vp), ("dt", _f64), ("dnu", _f64), ("do_tsmear", _i32), ("do_fsmear", _i32),
+        ("large_blocks", _vp), ("nlarge", _i64), ("large_min_vis", _i64),
     ]
 
 

@@ -183,13 +183,14 @@ def row_chunks(w: Workload, nchunks: int) -> List[pipeline.Chunk]:
 
 
 def uneven_bda(device=None, scale=1.0, seed=1003, nfacets=25, npix_image=6000, cell=1.0, nchan=128, nw=32,
-               grid_decorr=0.02, nsrc=200, block_order_tile=64):
+               grid_decorr=0.02, nsrc=200, block_order_tile=64, large_min_vis=256):
     """Uneven facets with baseline-dependent averaging: a 6000^2 image at 1"/pixel in a Voronoi
     tessellation around 25 directions, 48 antennas in a 12 km log-radial layout, 6 h at 4 s,
     128 channels 0.9-1.7 GHz, 4 correlations, per-facet per-antenna 5-min Jones; block map of
     DDFacet's default mode 1 with GridDecorr 0.02 over the largest facet's field, built on the
     GPU (every block averages a few rows and channels, more on short baselines), its blocks
-    visited in uv Z order (``block_order_tile`` cells per tile; 0 keeps the map order)."""
+    visited in uv Z order (``block_order_tile`` cells per tile; 0 keeps the map order) and blocks of
+    more than ``large_min_vis`` visibilities walked by a whole warp each (0: none)."""
     dev = D._dev(device)
     hours = 6.0 * scale
     obs = synth.make_observation(seed, 48, 12000.0, 34.0, 40.0, hours, 4.0, nchan, 0.90e9, 1.70e9, layout="lograd")
@@ -219,6 +220,8 @@ def uneven_bda(device=None, scale=1.0, seed=1003, nfacets=25, npix_image=6000, c
         tile = block_order_tile / (max(f.npix_padded for f in tess.facets) * tess.cell_rad)
         vs = vs.with_block_order(bda.uv_locality_order(vs.bda_map, vs.block_start, vs.uvw, vs.freqs, tile))
         del bmap
+    if large_min_vis:
+        vs = vs.with_large_blocks(large_min_vis)
     nt = int(np.ceil(hours * 3600 / 300.0))
     J = synth.random_jones(seed + 3, nt, nfacets, 48, 1, 0.1)
     tmap = np.minimum(((obs.times - obs.times.min()) // 300.0).astype(np.int32), nt - 1)
@@ -244,6 +247,8 @@ def uneven_bda(device=None, scale=1.0, seed=1003, nfacets=25, npix_image=6000, c
     w = Workload("uneven_bda", vs, fg, fm, jd, pol, nvis=nrow * nchan, nrow=nrow, nchan=nchan, ncorr=ncorr,
                  nfacets=len(fg))
     w.info = dict(npix=tess.npix, grids=[f.npix_padded for f in tess.facets], nw=nw, nblocks=vs.nblocks,
+                  large_blocks=(0 if vs.large_blocks is None else int(vs.large_blocks.numel())),
+                  large_min_vis=large_min_vis,
                   block_order=(f"uv Z order, tiles of {block_order_tile} cells" if block_order_tile else "map order"),
                   vis_per_block=nrow * nchan / max(vs.nblocks, 1), wmax=wmax, nant=48, ntimes=obs.ntimes)
     w.host = {"obs": obs, "wterms": wts, "tess": tess, "chan_map": chan_map}

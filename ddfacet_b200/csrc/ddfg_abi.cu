@@ -152,6 +152,11 @@ int check_common(const char *who, const ddfg_vis *vs, const ddfg_jones *js, cons
     if (f.max_support <= 0 || f.max_support > 63)
       return ddfg_set_error(DDFG_EINVAL, "%s: facet %d max_support %d outside [1, 63]", who, i, f.max_support);
   }
+  if (vs->nlarge < 0 || (vs->nlarge > 0 && (!vs->large_blocks || vs->large_min_vis < 1)))
+    return ddfg_set_error(DDFG_EINVAL, "%s: bad large-block list", who);
+  if (vs->nlarge > 0 && js && js->mode != 0 && js->scale_jones)
+    return ddfg_set_error(DDFG_EUNSUPPORTED, "%s: a large-block list needs Jones terms that do not depend on uv "
+                          "(no scale_jones)", who);
   if (vs->ncorr == 4 && ((uintptr_t)vs->vis & 15))
     return ddfg_set_error(DDFG_EINVAL, "%s: 4-correlation visibilities must be 16-byte aligned", who);
   if ((uintptr_t)vs->vis & 7) return ddfg_set_error(DDFG_EINVAL, "%s: visibilities must be 8-byte aligned", who);

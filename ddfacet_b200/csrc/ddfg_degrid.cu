@@ -46,6 +46,8 @@ __global__ void __launch_bounds__(256) degrid_kernel(const ddfg_vis vs, const dd
     const bool inrange = b < vs.nblocks;
     DegridBlock d;
     if (inrange && !SINGLE) degrid_block_header(vs, b, d);
+    // blocks of the large-block list are left to the second loop
+    const bool mine = inrange && (SINGLE || !(vs.nlarge > 0 && (int64_t)d.nrows * (d.ch1 - d.ch0) > vs.large_min_vis));
     for (int fi = 0; fi < pack.n; ++fi) {
       const ddfg_facet &f = sf[fi];
       BlockGeom g;
@@ -53,16 +55,34 @@ __global__ void __launch_bounds__(256) degrid_kernel(const ddfg_vis vs, const dd
       int64_t srow = 0;
       bool valid;
       if (SINGLE) valid = inrange && degrid_single_geom(vs, f, b, sch, srow, sgc, g);
-      else valid = inrange && degrid_block_geom(vs, f, d, g);
+      else valid = mine && degrid_block_geom(vs, f, d, g);
       TapJob job;
       if (valid) job = tap_job(g, SINGLE ? sgc : d.gridchan, f);
 
-      float2 mine[NPOL];
-      gather_records<NPOL, SLOTS>(valid, job, f, lt, wpart, lane, mine);
+      float2 pred[NPOL];
+      gather_records<NPOL, SLOTS>(valid, job, f, lt, wpart, lane, pred);
       if (valid) {
-        if (SINGLE) degrid_single_apply<NPOL>(vs, js, f, dp, sch, srow, mine);
-        else degrid_block_apply<NPOL>(vs, js, f, dp, d, mine);
+        if (SINGLE) degrid_single_apply<NPOL>(vs, js, f, dp, sch, srow, pred);
+        else degrid_block_apply<NPOL>(vs, js, f, dp, d, pred);
       }
+    }
+  }
+  if (SINGLE) return;
+  // Large blocks, one warp each: lane 0 forms the footprint (row means in the reference's
+  // order), the warp gathers the taps and applies the prediction to the block's visibilities
+  // lane-strided (degrid_block_apply_warp).
+  for (int64_t t = (int64_t)blockIdx.x * nwarps + warp; t < vs.nlarge; t += (int64_t)gridDim.x * nwarps) {
+    DegridBlock d;
+    degrid_block_header(vs, vs.large_blocks[t], d);
+    for (int fi = 0; fi < pack.n; ++fi) {
+      const ddfg_facet &f = sf[fi];
+      BlockGeom g;
+      const bool valid = lane == 0 && degrid_block_geom(vs, f, d, g);
+      TapJob job;
+      if (valid) job = tap_job(g, d.gridchan, f);
+      float2 pred[NPOL];
+      gather_records<NPOL, SLOTS>(valid, job, f, lt, wpart, lane, pred);
+      if (__shfl_sync(0xffffffffu, valid, 0)) degrid_block_apply_warp<NPOL>(vs, js, f, dp, d, pred, 0, lane);
     }
   }
 }

@@ -59,54 +59,108 @@ __device__ __forceinline__ bool degrid_block_geom(const ddfg_vis &vs, const ddfg
   return block_geometry(f, um, vm, wm, rw, g);
 }
 
-// Stokes prediction -> correlations, Jones, smearing, phasor; subtract from the visibilities.
+// The block's Stokes -> correlation prediction with the per-block Jones (BDAJones), smearing
+// factor and facet term n0 - 1: what every visibility of the block is derived from.
+struct DegridBlockPred {
+  M2 corr_vis;
+  float dec;
+  double n0m1;
+};
+
 template <int NPOL>
-__device__ __forceinline__ void degrid_block_apply(const ddfg_vis &vs, const ddfg_jones &js, const ddfg_facet &f,
-                                                   const DegridParams &dp, const DegridBlock &d, const float2 *pred) {
+__device__ __forceinline__ DegridBlockPred degrid_block_pred(const ddfg_vis &vs, const ddfg_jones &js,
+                                                             const ddfg_facet &f, const DegridParams &dp,
+                                                             const DegridBlock &d, const float2 *pred,
+                                                             JonesCache &jc) {
   float2 s[4];
 #pragma unroll
   for (int p = 0; p < 4; ++p) s[p] = (p < NPOL) ? pred[p] : czero();
-  M2 corr_vis = corr_from_stokes(dp.policy, s);
-  JonesCache jc;
+  DegridBlockPred bp;
+  bp.corr_vis = corr_from_stokes(dp.policy, s);
   jc.reset();
   const int mid = d.rows[d.nrows / 2];
   if (js.mode == 2) {
     const double *up = vs.uvw + 3 * (int64_t)mid;
     jc.update(js, f.idir_kms, f.idir_beam, mid, (d.ch0 + d.ch1) / 2, up[0], up[1]);
-    corr_vis = m2_times(m2_times(jc.j0, corr_vis), m2_herm(jc.j1));
+    bp.corr_vis = m2_times(m2_times(jc.j0, bp.corr_vis), m2_herm(jc.j1));
   }
-  const float dec = (float)decorr_factor(vs, f, d.freqmean, mid);
-  const double n0m1 = sqrt(1. - f.l0 * f.l0 - f.m0 * f.m0) - 1.;
-  const int nchan = vs.nchan, ncorr = vs.ncorr;
-  float2 *visd = (float2 *)vs.vis;
+  bp.dec = (float)decorr_factor(vs, f, d.freqmean, mid);
+  bp.n0m1 = sqrt(1. - f.l0 * f.l0 - f.m0 * f.m0) - 1.;
+  return bp;
+}
+
+// One visibility of a block: per-visibility Jones, phasor exp(+i nu angle) and smearing, then
+// vis -= (subtractVis<nVisCorr>, degridder.h:43-53, 227-261).
+__device__ __forceinline__ void degrid_vis_update(const ddfg_vis &vs, const ddfg_jones &js, const ddfg_facet &f,
+                                                  const DegridBlockPred &bp, int64_t irow, int ch,
+                                                  JonesCache &jc) {
+  const double *up = vs.uvw + 3 * irow;
+  const double dot = up[0] * f.l0 + up[1] * f.m0 + up[2] * bp.n0m1;
+  const float2 ph = cscale(phasor_turns(vs.freqs[ch] * dot * kInvC), bp.dec);
+  M2 vb;
+  if (js.mode == 1) {
+    jc.update(js, f.idir_kms, f.idir_beam, irow, ch, up[0], up[1]);
+    vb = m2_scale(m2_times(m2_times(jc.j0, bp.corr_vis), m2_herm(jc.j1)), ph);
+  } else {
+    vb = m2_scale(bp.corr_vis, ph);
+  }
+  float2 *vp = (float2 *)vs.vis + (irow * vs.nchan + ch) * (int64_t)vs.ncorr;
+  if (vs.ncorr == 4) {
+    float4 a = *(float4 *)vp, c = *(float4 *)(vp + 2);
+    a.x -= vb.v[0].x; a.y -= vb.v[0].y; a.z -= vb.v[1].x; a.w -= vb.v[1].y;
+    c.x -= vb.v[2].x; c.y -= vb.v[2].y; c.z -= vb.v[3].x; c.w -= vb.v[3].y;
+    *(float4 *)vp = a;
+    *(float4 *)(vp + 2) = c;
+  } else if (vs.ncorr == 2) {
+    vp[0] = csub(vp[0], vb.v[0]);
+    vp[1] = csub(vp[1], vb.v[3]);
+  } else {
+    vp[0] = csub(vp[0], vb.v[0]);
+  }
+}
+
+// Stokes prediction -> correlations, Jones, smearing, phasor; subtract from the visibilities.
+template <int NPOL>
+__device__ __forceinline__ void degrid_block_apply(const ddfg_vis &vs, const ddfg_jones &js, const ddfg_facet &f,
+                                                   const DegridParams &dp, const DegridBlock &d, const float2 *pred) {
+  JonesCache jc;
+  const DegridBlockPred bp = degrid_block_pred<NPOL>(vs, js, f, dp, d, pred, jc);
   for (int inx = 0; inx < d.nrows; ++inx) {
     const int64_t irow = d.rows[inx];
-    const double *up = vs.uvw + 3 * irow;
-    const double dot = up[0] * f.l0 + up[1] * f.m0 + up[2] * n0m1;
-    for (int ch = d.ch0; ch < d.ch1; ++ch) {
-      const float2 ph = cscale(phasor_turns(vs.freqs[ch] * dot * kInvC), dec);
-      M2 vb;
-      if (js.mode == 1) {
-        jc.update(js, f.idir_kms, f.idir_beam, irow, ch, up[0], up[1]);
-        vb = m2_scale(m2_times(m2_times(jc.j0, corr_vis), m2_herm(jc.j1)), ph);
-      } else {
-        vb = m2_scale(corr_vis, ph);
-      }
-      float2 *vp = visd + (irow * nchan + ch) * (int64_t)ncorr;
-      // subtractVis<nVisCorr> (degridder.h:43-53)
-      if (ncorr == 4) {
-        float4 a = *(float4 *)vp, c = *(float4 *)(vp + 2);
-        a.x -= vb.v[0].x; a.y -= vb.v[0].y; a.z -= vb.v[1].x; a.w -= vb.v[1].y;
-        c.x -= vb.v[2].x; c.y -= vb.v[2].y; c.z -= vb.v[3].x; c.w -= vb.v[3].y;
-        *(float4 *)vp = a;
-        *(float4 *)(vp + 2) = c;
-      } else if (ncorr == 2) {
-        vp[0] = csub(vp[0], vb.v[0]);
-        vp[1] = csub(vp[1], vb.v[3]);
-      } else {
-        vp[0] = csub(vp[0], vb.v[0]);
-      }
-    }
+    for (int ch = d.ch0; ch < d.ch1; ++ch) degrid_vis_update(vs, js, f, bp, irow, ch, jc);
+  }
+}
+
+// degrid_block_apply of lane src's block by the whole warp (all 32 lanes call it): lanes take the
+// block's visibilities in row-major order, lane-strided.  Every visibility's update is
+// independent, and with uv-independent Jones terms (no DoScaleJones) a lane's own cache gives the
+// values the owner's walk would, so the result is the same.
+template <int NPOL>
+__device__ __forceinline__ void degrid_block_apply_warp(const ddfg_vis &vs, const ddfg_jones &js,
+                                                        const ddfg_facet &f, const DegridParams &dp,
+                                                        const DegridBlock &own, const float2 *own_pred, int src,
+                                                        int lane) {
+  DegridBlock d;
+  d.start = __shfl_sync(0xffffffffu, own.start, src);
+  d.nrows = __shfl_sync(0xffffffffu, own.nrows, src);
+  d.ch0 = __shfl_sync(0xffffffffu, own.ch0, src);
+  d.ch1 = __shfl_sync(0xffffffffu, own.ch1, src);
+  d.gridchan = __shfl_sync(0xffffffffu, own.gridchan, src);
+  d.freqmean = __shfl_sync(0xffffffffu, own.freqmean, src);
+  d.rows = vs.bda_map + d.start + 2;
+  float2 pred[NPOL];
+#pragma unroll
+  for (int p = 0; p < NPOL; ++p) {
+    pred[p].x = __shfl_sync(0xffffffffu, own_pred[p].x, src);
+    pred[p].y = __shfl_sync(0xffffffffu, own_pred[p].y, src);
+  }
+  JonesCache jc;
+  const DegridBlockPred bp = degrid_block_pred<NPOL>(vs, js, f, dp, d, pred, jc);
+  const int nch = d.ch1 - d.ch0;
+  const int64_t total = (int64_t)d.nrows * nch;
+  for (int64_t k = lane; k < total; k += 32) {
+    const int inx = (int)(k / nch);
+    degrid_vis_update(vs, js, f, bp, d.rows[inx], d.ch0 + (int)(k - (int64_t)inx * nch), jc);
   }
 }
 

@@ -112,15 +112,38 @@ __global__ void __launch_bounds__(128, 3) grid_block_fi_kernel(const ddfg_vis vs
   lt.reset();
   for (int64_t s = (int64_t)blockIdx.x * nwarps + warp; s < nstripes; s += (int64_t)gridDim.x * nwarps) {
     const int64_t b = s * 32 + lane;
+    // blocks of the large-block list are left to the second loop
+    const bool mine = b < vs.nblocks && !(vs.nlarge > 0 && block_nvis(vs, b) > vs.large_min_vis);
     for (int fi = 0; fi < pack.n; ++fi) {
       const ddfg_facet &f = sf[fi];
       const int npol_used = min(gp.nvispol, f.npol);
       double *a = s_acc + (size_t)fi * acc_stride;
       GridRecord<NPOL> rec;
       rec.valid = false;
-      if (b < vs.nblocks) grid_block_record<NPOL>(vs, js, f, gp, b, s_n0m1[fi], rec, jc);
+      if (mine) grid_block_record<NPOL>(vs, js, f, gp, b, s_n0m1[fi], rec, jc);
       warp_add_block_sums<NPOL, false>(vs, js, f, gp, b, rec, npol_used, a, a + f.nband * f.npol,
                                        a + f.nband * f.npol + 2 * f.nband, jc);
+      scatter_records<NPOL, SLOTS>(rec, f, npol_used, lt, lane);
+    }
+  }
+  // Large blocks, one warp each: lane 0 walks the FP64 means in the reference's order, the warp
+  // the rest (grid_block_record_warp); lane 0 holds the record the warp then lays down.
+  for (int64_t t = (int64_t)blockIdx.x * nwarps + warp; t < vs.nlarge; t += (int64_t)gridDim.x * nwarps) {
+    const int64_t bl = vs.large_blocks[t];
+    if (vs.sparsification && !vs.sparsification[bl]) continue;
+    for (int fi = 0; fi < pack.n; ++fi) {
+      const ddfg_facet &f = sf[fi];
+      const int npol_used = min(gp.nvispol, f.npol);
+      double *a = s_acc + (size_t)fi * acc_stride;
+      double *a_chan = a + f.nband * f.npol + 2 * f.nband;
+      BlockMeans bm{};
+      if (lane == 0) bm = grid_block_means(vs, f, bl);
+      GridRecord<NPOL> rec;
+      rec.valid = false;
+      rec.single_chan = true;
+      grid_block_record_warp<NPOL>(vs, js, f, gp, bl, bm, s_n0m1[fi], 0, lane, npol_used, a_chan, rec);
+      warp_add_block_sums<NPOL, false>(vs, js, f, gp, bl, rec, npol_used, a, a + f.nband * f.npol, a_chan, jc,
+                                       !rec.single_chan);
       scatter_records<NPOL, SLOTS>(rec, f, npol_used, lt, lane);
     }
   }

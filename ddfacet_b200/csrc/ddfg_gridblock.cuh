@@ -327,7 +327,7 @@ template <int NPOL, bool SINGLE = false>
 __device__ __forceinline__ void warp_add_block_sums(const ddfg_vis &vs, const ddfg_jones &js, const ddfg_facet &f,
                                                     const GridParams &gp, int64_t b, const GridRecord<NPOL> &rec,
                                                     int npol_used, double *a_sumwt, double *a_sumj, double *a_chan,
-                                                    JonesCache &jc) {
+                                                    JonesCache &jc, bool chan_sums_done = false) {
   const unsigned vmask = __ballot_sync(0xffffffffu, rec.valid);
   if (!vmask) return;
   const int lane = threadIdx.x & 31;
@@ -352,13 +352,222 @@ __device__ __forceinline__ void warp_add_block_sums(const ddfg_vis &vs, const dd
       atomicAdd(&a_sumj[f.nband + g], (double)npol_used * qsum);
     }
   }
-  if (js.mode != 0 && rec.valid) {
+  if (js.mode != 0 && rec.valid && !chan_sums_done) {
     if (SINGLE) {
       atomicAdd(&a_chan[rec.ch0], (double)npol_used * rec.sumjones);
       atomicAdd(&a_chan[vs.nchan + rec.ch0], (double)npol_used * rec.sumsqw);
     } else {
       grid_block_add_chan_sums<NPOL>(vs, js, f, gp, b, rec, (double)npol_used, a_chan, jc);
     }
+  }
+}
+
+// Visibilities of block b (rows x channels, flagged ones included).
+__device__ __forceinline__ int64_t block_nvis(const ddfg_vis &vs, int64_t b) {
+  const int64_t start = vs.block_start[b];
+  return (int64_t)(vs.bda_map[2 + b] - 2) * (vs.bda_map[start + 1] - vs.bda_map[start]);
+}
+
+// The FP64 block means of grid_block_record in the reference's order (gridder.h:272-279): one
+// lane, only the flags read per visibility.  Keeping this sum sequential keeps every integer index
+// derived from it bit-exact.
+struct BlockMeans {
+  double u, v, w, nu;
+  int nvis, last_ch;
+};
+
+__device__ __forceinline__ BlockMeans grid_block_means(const ddfg_vis &vs, const ddfg_facet &f, int64_t b) {
+  BlockMeans m;
+  m.u = m.v = m.w = m.nu = 0.;
+  m.nvis = 0;
+  const int64_t start = vs.block_start[b];
+  const int nrows_blk = vs.bda_map[2 + b] - 2;
+  const int ch0 = vs.bda_map[start], ch1 = vs.bda_map[start + 1];
+  m.last_ch = ch0;
+  const int32_t *rows = vs.bda_map + start + 2;
+  for (int inx = 0; inx < nrows_blk; ++inx) {
+    const int64_t irow = rows[inx];
+    const double *up = vs.uvw + 3 * irow;
+    const double W = up[2];
+    const double tu = dadd(up[0], dmul(W, f.cu)), tv = dadd(up[1], dmul(W, f.cv));
+    const unsigned char *fl = vs.flags + irow * vs.nchan * (int64_t)vs.ncorr;
+    for (int ch = ch0; ch < ch1; ++ch) {
+      if (fl[(int64_t)ch * vs.ncorr]) continue;
+      m.u = dadd(m.u, tu);
+      m.v = dadd(m.v, tv);
+      m.w = dadd(m.w, W);
+      m.nu = dadd(m.nu, vs.freqs[ch]);
+      m.last_ch = ch;
+      ++m.nvis;
+    }
+  }
+  return m;
+}
+
+__device__ __forceinline__ double warp_sum(double x) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+  return x;
+}
+
+__device__ __forceinline__ float warp_sum(float x) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+  return x;
+}
+
+// grid_block_record of lane src's block b by the whole warp (all 32 lanes call it; the Jones
+// terms must not depend on uv, i.e. no DoScaleJones): lanes take the block's visibilities in
+// row-major order, lane-strided, and the weighted visibility and weight sums are reduced across
+// the warp; the FP64 means come from the owner's sequential walk (grid_block_means, passed in by
+// lane src).  With uv-independent Jones terms every lane's cache gives the owner's values.  Lane src receives the record.  When the
+// block is valid and carries Jones sums over several channels, the per-channel sums are added to
+// a_chan here (the caller passes chan_sums_done to warp_add_block_sums).
+template <int NPOL>
+__device__ __forceinline__ void grid_block_record_warp(const ddfg_vis &vs, const ddfg_jones &js, const ddfg_facet &f,
+                                                       const GridParams &gp, int64_t b_own, const BlockMeans &m_own,
+                                                       double n0m1, int src, int lane, int npol_used, double *a_chan,
+                                                       GridRecord<NPOL> &rec) {
+  const int64_t b = __shfl_sync(0xffffffffu, b_own, src);
+  BlockMeans bm;
+  bm.u = __shfl_sync(0xffffffffu, m_own.u, src);
+  bm.v = __shfl_sync(0xffffffffu, m_own.v, src);
+  bm.w = __shfl_sync(0xffffffffu, m_own.w, src);
+  bm.nu = __shfl_sync(0xffffffffu, m_own.nu, src);
+  bm.nvis = __shfl_sync(0xffffffffu, m_own.nvis, src);
+  bm.last_ch = __shfl_sync(0xffffffffu, m_own.last_ch, src);
+  const int64_t start = vs.block_start[b];
+  const int nrows_blk = vs.bda_map[2 + b] - 2;
+  const int ch0 = vs.bda_map[start], ch1 = vs.bda_map[start + 1];
+  const int32_t *rows = vs.bda_map + start + 2;
+  const int nchan = vs.nchan, ncorr = vs.ncorr;
+  const int nch = ch1 - ch0;
+  const int64_t total = (int64_t)nrows_blk * nch;
+  const double dec = decorr_factor(vs, f, gp.freq_mean0, rows[nrows_blk / 2]);
+  const float decf = (float)dec;
+  JonesCache jc;
+  jc.reset();
+  M2 vis_acc;
+#pragma unroll
+  for (int p = 0; p < 4; ++p) vis_acc.v[p] = czero();
+  M2 vmeas;
+  vmeas.v[0] = make_float2(decf, 0.f);
+  vmeas.v[1] = czero();
+  vmeas.v[2] = czero();
+  vmeas.v[3] = make_float2(decf, 0.f);
+  bool have_psf = false;
+  double thisweight = 0., sumjones = 0., sumsqw = 0.;
+  const float2 *visd = (const float2 *)vs.vis;
+  for (int64_t k = lane; k < total; k += 32) {
+    const int inx = (int)(k / nch);
+    const int ch = ch0 + (int)(k - (int64_t)inx * nch);
+    const int64_t irow = rows[inx];
+    const int64_t doff = (irow * nchan + ch) * (int64_t)ncorr;
+    if (vs.flags[doff]) continue;
+    const double *up = vs.uvw + 3 * irow;
+    const double U = up[0], V = up[1], W = up[2];
+    const double dot = U * f.l0 + V * f.m0 + W * n0m1;
+    const double nu = vs.freqs[ch];
+    const float2 corr = gp.dopsf ? make_float2(1.f, 0.f) : phasor_turns(-nu * dot * kInvC);
+    if (js.mode == 1) {
+      const bool chg = jc.update(js, f.idir_kms, f.idir_beam, irow, ch, U, V);
+      if ((chg || !have_psf) && gp.dopsf) {
+        vmeas = m2_times(jc.j0, m2_herm(jc.j1));
+        vmeas = m2_times(m2_times(m2_herm(jc.j0), vmeas), jc.j1);
+        vmeas = m2_scale(vmeas, make_float2(decf, 0.f));
+        have_psf = true;
+      }
+    }
+    if (!gp.dopsf) {
+      const float2 *vp = visd + doff;
+      if (ncorr == 4) {
+        vmeas.v[0] = vp[0]; vmeas.v[1] = vp[1]; vmeas.v[2] = vp[2]; vmeas.v[3] = vp[3];
+      } else if (ncorr == 2) {
+        vmeas.v[0] = vp[0]; vmeas.v[1] = czero(); vmeas.v[2] = czero(); vmeas.v[3] = vp[1];
+      } else {
+        vmeas.v[0] = vp[0]; vmeas.v[1] = czero(); vmeas.v[2] = czero(); vmeas.v[3] = vp[0];
+      }
+    }
+    const double fw = (double)vs.weights[irow * nchan + ch];
+    const float2 wgt = cscale(corr, (float)fw);
+    const double fwd = fw * dec * dec;
+    sumsqw += fwd;
+    if (js.mode == 1) {
+      if (!gp.dopsf) vmeas = m2_times(m2_times(m2_herm(jc.j0), vmeas), jc.j1);
+      sumjones += (double)jc.bb * fwd;
+    }
+    vis_acc.v[0] = cadd(vis_acc.v[0], cmul(vmeas.v[0], wgt));
+    if (ncorr == 4) {
+      vis_acc.v[1] = cadd(vis_acc.v[1], cmul(vmeas.v[1], wgt));
+      vis_acc.v[2] = cadd(vis_acc.v[2], cmul(vmeas.v[2], wgt));
+    }
+    if (ncorr >= 2) vis_acc.v[3] = cadd(vis_acc.v[3], cmul(vmeas.v[3], wgt));
+    thisweight += fw;
+  }
+#pragma unroll
+  for (int p = 0; p < 4; ++p) {
+    vis_acc.v[p].x = warp_sum(vis_acc.v[p].x);
+    vis_acc.v[p].y = warp_sum(vis_acc.v[p].y);
+  }
+  thisweight = warp_sum(thisweight);
+  sumsqw = warp_sum(sumsqw);
+  if (js.mode == 1) sumjones = warp_sum(sumjones);
+  if (bm.nvis == 0) return;
+  double umean = bm.u, vmean = bm.v, wmean = bm.w, freqmean = bm.nu;
+  if (bm.nvis > 1) {
+    const double dn = (double)bm.nvis;
+    umean = umean / dn;
+    vmean = vmean / dn;
+    wmean = wmean / dn;
+    freqmean = freqmean / dn;
+  }
+  if (js.mode == 2) {
+    jc.reset();
+    jc.update(js, f.idir_kms, f.idir_beam, rows[nrows_blk / 2], (ch0 + ch1) / 2, umean, vmean);
+    if (gp.dopsf) vis_acc = m2_times(m2_times(jc.j0, vis_acc), m2_herm(jc.j1));
+    vis_acc = m2_times(m2_times(m2_herm(jc.j0), vis_acc), jc.j1);
+    sumjones = sumsqw * (double)jc.bb;
+  }
+  const int gridchan = vs.chan_map[ch0];
+  if (gridchan < 0 || gridchan >= f.nband) return;
+  const double recip_wvl = (bm.nvis == 1 && vs.recip_wvl) ? vs.recip_wvl[bm.last_ch] : freqmean / kC;
+  BlockGeom g;
+  if (!block_geometry(f, umean, vmean, wmean, recip_wvl, g)) return;
+  // per-channel Jones sums of the valid block (grid_block_chan_sums), lane-strided
+  if (js.mode != 0 && nch > 1) {
+    const float block_bb = jc.bb;
+    JonesCache jc2;
+    jc2.reset();
+    const double mult = (double)npol_used;
+    for (int64_t k = lane; k < total; k += 32) {
+      const int inx = (int)(k / nch);
+      const int ch = ch0 + (int)(k - (int64_t)inx * nch);
+      const int64_t irow = rows[inx];
+      if (vs.flags[(irow * nchan + ch) * (int64_t)ncorr]) continue;
+      const double fwd = (double)vs.weights[irow * nchan + ch] * dec * dec;
+      double bbv = (double)block_bb;
+      if (js.mode == 1) {
+        const double *up = vs.uvw + 3 * irow;
+        jc2.update(js, f.idir_kms, f.idir_beam, irow, ch, up[0], up[1]);
+        bbv = (double)jc2.bb;
+      }
+      atomicAdd(&a_chan[ch], mult * bbv * fwd);
+      atomicAdd(&a_chan[nchan + ch], mult * fwd);
+    }
+  }
+  if (lane == src) {
+    float2 st[4];
+    stokes_from_corr(gp.policy, vis_acc, st);
+#pragma unroll
+    for (int p = 0; p < NPOL; ++p) rec.stokes[p] = st[p];
+    rec.g = g;
+    rec.valid = true;
+    rec.gridchan = gridchan;
+    rec.weight = thisweight;
+    rec.sumjones = sumjones;
+    rec.sumsqw = sumsqw;
+    rec.ch0 = ch0;
+    rec.single_chan = (nch == 1);
   }
 }
 

@@ -78,6 +78,8 @@ class VisData:
     dnu: float = 0.0
     do_tsmear: int = 0
     do_fsmear: int = 0
+    large_blocks: Optional[torch.Tensor] = None   # int64 [nlarge] (with_large_blocks)
+    large_min_vis: int = 0
 
     @staticmethod
     def plan_map(bda_map: torch.Tensor, nrow: int, nchan: int, stream=None):
@@ -159,7 +161,26 @@ class VisData:
         m = bda.reorder_blocks(self.bda_map, self.block_start, order)
         starts, single = self.plan_map(m, int(self.vis.shape[0]), int(self.vis.shape[1]))
         sp = None if self.sparsification is None else self.sparsification[order].contiguous()
-        return replace(self, bda_map=m, block_start=starts, single_vis_blocks=single, sparsification=sp)
+        out = replace(self, bda_map=m, block_start=starts, single_vis_blocks=single, sparsification=sp,
+                      large_blocks=None, large_min_vis=0)
+        return out.with_large_blocks(self.large_min_vis) if self.large_blocks is not None else out
+
+    def with_large_blocks(self, min_vis: int = 128) -> "VisData":
+        """The same visibilities with the list of blocks of more than ``min_vis`` visibilities
+        (rows x channels) that the averaged-block kernels give a whole warp each (ddfg_vis
+        large_blocks).  Mode-1 maps give the shortest baselines blocks spanning the whole track;
+        one lane per block would hold its warp for the whole walk.  Needs Jones terms that do
+        not depend on uv (no scale_jones)."""
+        if min_vis < 1:
+            raise ValueError("min_vis must be positive")
+        nb = self.nblocks
+        if nb == 0 or self.single_vis_blocks:
+            return replace(self, large_blocks=None, large_min_vis=0)
+        sizes = self.bda_map[2:2 + nb].to(torch.int64) - 2
+        st = self.block_start
+        nv = sizes * (self.bda_map[st + 1].to(torch.int64) - self.bda_map[st].to(torch.int64))
+        idx = torch.nonzero(nv > int(min_vis)).flatten().contiguous()
+        return replace(self, large_blocks=idx if idx.numel() else None, large_min_vis=int(min_vis))
 
     def struct(self) -> _abi.VisSet:
         s = _abi.VisSet()
@@ -183,6 +204,10 @@ class VisData:
         s.uvw_dt = _ptr(self.uvw_dt)
         s.dt, s.dnu = self.dt, self.dnu
         s.do_tsmear, s.do_fsmear = self.do_tsmear, self.do_fsmear
+        if self.large_blocks is not None and self.large_blocks.numel() > 0:
+            s.large_blocks = self.large_blocks.data_ptr()
+            s.nlarge = int(self.large_blocks.numel())
+            s.large_min_vis = int(self.large_min_vis)
         return s
 
 

@@ -90,6 +90,15 @@ typedef struct ddfg_vis {
   const double *uvw_dt;        /* [nrow][3]                                               */
   double dt, dnu;
   int32_t do_tsmear, do_fsmear;
+  /* Large blocks (optional; nlarge 0 disables): large_blocks[nlarge] must list, in any order,
+     exactly the blocks of more than large_min_vis visibilities (rows x channels).  The
+     averaged-block kernels of ddfg_grid / ddfg_degrid take them out of the one-lane-per-block
+     walks and give each to one warp, its lanes strided over the block's visibilities; the
+     FP64 block means keep the reference's sequential order, so indices stay bit-exact.
+     Needs Jones terms that do not depend on uv (no scale_jones). */
+  const int64_t *large_blocks;
+  int64_t nlarge;
+  int64_t large_min_vis;
 } ddfg_vis;
 
 /* Direction-dependent Jones terms (LJones, ClassDDEGridMachine.py:665-677). */

@@ -70,3 +70,25 @@ def test_uv_locality_order():
     # with W planes as the second key, planes never decrease inside a tile
     ow = bda.uv_locality_order(m, starts, uvw, fr, tile, w_planes=(4, float(np.abs(c.uvw[:, 2]).max()) * 1.01))
     assert sorted(ow.tolist()) == list(range(nb))
+
+
+def test_large_block_list_rule():
+    """VisData.with_large_blocks lists exactly the blocks of more than min_vis visibilities (the
+    rule the kernels use to leave them out of the one-lane walks); block reordering rebuilds it."""
+    from ddfacet_b200 import device as D
+
+    c = cases.make_case(seed=5, bda_mode=1, dphi=np.sqrt(6 * 1.0), nchan=16, ntimes=60, ncorr=4)
+    m = torch.from_numpy(c.bda)
+    starts = _starts(c.bda)
+    nb = starts.numel()
+    blocks = _blocks(c.bda)
+    nv = np.array([(len(b) - 2) * (b[1] - b[0]) for b in blocks])
+    vs = D.VisData(vis=torch.zeros((c.nrow, c.nchan, 4), dtype=torch.complex64), uvw=torch.from_numpy(c.uvw),
+                   flags=torch.zeros((c.nrow, c.nchan, 4), dtype=torch.uint8),
+                   weights=torch.ones((c.nrow, c.nchan)), freqs=torch.from_numpy(c.freqs), freqs_host=c.freqs,
+                   recip_wvl=torch.from_numpy(c.freqs / 299792458.0), chan_map=torch.zeros(c.nchan, dtype=torch.int32),
+                   bda_map=m, block_start=starts, nblocks=nb, chan_equidistant=1)
+    big = vs.with_large_blocks(128)
+    np.testing.assert_array_equal(big.large_blocks.numpy(), np.flatnonzero(nv > 128))
+    assert big.large_min_vis == 128 and big.struct().nlarge == int((nv > 128).sum())
+    assert vs.with_large_blocks(10 ** 6).large_blocks is None

@@ -120,6 +120,55 @@ def test_large_blocks(jmode, psf, scale):
         _cmp_degrid(c)
 
 
+@pytest.mark.parametrize("jmode,psf,sparse", [(0, False, True), (1, False, False), (2, False, False), (1, True, False),
+                                              (2, True, True)])
+def test_large_block_list(jmode, psf, sparse):
+    """Blocks of more than 128 visibilities given a whole warp each (VisData.with_large_blocks,
+    ddfg_vis large_blocks): grid, touched cells, weight and Jones sums and prediction against the
+    reference, with a sparsification mask in some cases."""
+    import torch
+
+    from ddfacet_b200 import device as D
+
+    c = cases.make_case(bda_mode=1, dphi=np.sqrt(6 * 1.0), nchan=16, ntimes=60, flag_frac=0.1, ncorr=4)
+    if jmode:
+        cases.add_jones(c, mode=jmode, nt=3, nd=3)
+    nb = int(np.uint32(c.bda[0]))
+    sp = (np.random.default_rng(2).uniform(size=nb) < 0.7) if sparse else None
+    r = cases.run_ref_grid(c, dopsf=psf, sparsification=sp)
+    pol = D.make_pol(c.corr_ids, c.stokes_ids)
+    vs, fg, jd = cases._gpu_objs(c)
+    if sparse:
+        vs.sparsification = torch.from_numpy(sp.astype(np.uint8)).cuda()
+    vs = vs.with_large_blocks(128)
+    assert vs.large_blocks is not None and vs.large_blocks.numel() >= 32
+    D.grid(vs, [fg], pol, jd, dopsf=psf)
+    g = fg.grid.cpu().numpy()
+    assert cases.rel_rms(g, r["grid"]) < TOL
+    np.testing.assert_array_equal(g != 0, r["grid"] != 0)
+    np.testing.assert_allclose(fg.sumwt.cpu().numpy(), r["sumwt"], rtol=1e-9)
+    if jmode:
+        np.testing.assert_allclose(fg.sumjones.cpu().numpy(), r["sumjones"], rtol=1e-5)
+        np.testing.assert_allclose(fg.sumjones_chan.cpu().numpy(), r["sumjones_chan"], rtol=1e-5)
+    if not psf:
+        model = cases.run_ref_grid(c)["grid"]
+        vr = cases.run_ref_degrid(c, model, vis0=c.vis)
+        vs2, fm, jd2 = cases._gpu_objs(c, model_grid=model)
+        vs2 = vs2.with_large_blocks(128)
+        D.degrid(vs2, [fm], pol, jd2)
+        assert cases.rel_rms(c.vis - vs2.vis.cpu().numpy(), c.vis - vr) < TOL
+
+
+def test_large_block_list_needs_uv_independent_jones():
+    from ddfacet_b200 import device as D
+
+    c = cases.make_case(bda_mode=1, dphi=np.sqrt(6 * 1.0), nchan=16, ntimes=60, ncorr=4)
+    cases.add_jones(c, mode=1, nt=3, nd=3, scale=1, calib_err=0.05)
+    vs, fg, jd = cases._gpu_objs(c)
+    with pytest.raises(ValueError, match="large-block list"):
+        D.grid(vs.with_large_blocks(128), [fg], D.make_pol(c.corr_ids, c.stokes_ids), jd)
+
+
 @pytest.mark.parametrize("jmode", [0, 1, 2])
 def test_bda_blocks_in_uv_order(jmode):
     """The blocks of a mode-1 map visited in uv Z order (VisData.with_block_order): grid, weight
