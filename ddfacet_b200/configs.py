@@ -183,7 +183,7 @@ def row_chunks(w: Workload, nchunks: int) -> List[pipeline.Chunk]:
 
 
 def uneven_bda(device=None, scale=1.0, seed=1003, nfacets=25, npix_image=6000, cell=1.0, nchan=128, nw=32,
-               grid_decorr=0.02, nsrc=200, block_order_tile=64, large_min_vis=256):
+               grid_decorr=0.02, nsrc=200, block_order_tile=64, large_min_vis=2048):
     """Uneven facets with baseline-dependent averaging: a 6000^2 image at 1"/pixel in a Voronoi
     tessellation around 25 directions, 48 antennas in a 12 km log-radial layout, 6 h at 4 s,
     128 channels 0.9-1.7 GHz, 4 correlations, per-facet per-antenna 5-min Jones; block map of
