@@ -176,7 +176,8 @@ int ddfg_launch_degrid(const ddfg_vis *vs, const ddfg_jones *js, const ddfg_face
 #define LAUNCH_D1(NP, SL)                                                                                          \
   do {                                                                                                             \
     cudaFuncSetAttribute(degrid_kernel<NP, SL, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);    \
-    degrid_kernel<NP, SL, false><<<num_ctas, 256, smem, stream>>>(*vs, *js, pack, dp);                             \
+    degrid_kernel<NP, SL, false><<<ddfg_one_wave(degrid_kernel<NP, SL, false>, 256, smem), 256, smem, stream>>>( \
+        *vs, *js, pack, dp);                                                                                       \
   } while (0)
 #define LAUNCH_DS(NP, SL)                                                                                          \
   do {                                                                                                             \

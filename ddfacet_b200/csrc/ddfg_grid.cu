@@ -262,7 +262,8 @@ int ddfg_launch_grid(const ddfg_vis *vs, const ddfg_jones *js, const ddfg_facet 
   do {                                                                                                             \
     if (smem_fi > 48 * 1024)                                                                                       \
       cudaFuncSetAttribute(grid_block_fi_kernel<NP, SL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_fi); \
-    grid_block_fi_kernel<NP, SL><<<2 * num_ctas, 128, smem_fi, stream>>>(*vs, *js, pack, gp, acc_stride);             \
+    grid_block_fi_kernel<NP, SL><<<ddfg_one_wave(grid_block_fi_kernel<NP, SL>, 128, smem_fi), 128, smem_fi, stream>>>( \
+        *vs, *js, pack, gp, acc_stride);                                                                           \
   } while (0)
 #define LAUNCH_B_NP(SL)              \
   switch (npol) {                    \

@@ -9,6 +9,17 @@ int ddfg_set_error(int code, const char *fmt, ...);
 // CTAs for a persistent launch on the current device (a multiple of the SM count).
 int ddfg_num_ctas(int ctas_per_sm);
 
+// One wave of a kernel: as many CTAs as can be resident at once on the current device (SMs x
+// resident CTAs per SM), for grid-stride kernels whose CTAs do unequal work -- with more CTAs
+// than fit, the later ones start as earlier ones finish and the last, partial wave sets the end.
+template <typename K>
+int ddfg_one_wave(K kernel, int threads, size_t smem) {
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem) != cudaSuccess || per_sm < 1)
+    per_sm = 1;
+  return ddfg_num_ctas(per_sm);
+}
+
 int ddfg_launch_grid(const ddfg_vis *vs, const ddfg_jones *js, const ddfg_facet *facets, int nfacets, int policy,
                      int nvispol, int dopsf, int num_ctas, cudaStream_t stream);
 int ddfg_launch_degrid(const ddfg_vis *vs, const ddfg_jones *js, const ddfg_facet *facets, int nfacets, int policy,
