@@ -20,6 +20,7 @@ DDFG_EMAP = -4
 DDFG_ESIZE = -5
 DDFG_MAX_FACETS = 1024
 DDFG_FACETS_PER_LAUNCH = 16
+DDFG_TABLE_FACETS = 128
 
 _i32 = C.c_int32
 _i64 = C.c_int64
@@ -40,6 +41,7 @@ class Facet(C.Structure):
         ("idir_kms", _i32), ("idir_beam", _i32),
         ("decorr_l", _f64), ("decorr_m", _f64),
         ("sumwt", _vp), ("sumjones", _vp), ("sumjones_chan", _vp),
+        ("grid_lo", _vp),
     ]
 
 
@@ -71,8 +73,9 @@ class Jones(C.Structure):
     ]
 
 
-class SortPlan(C.Structure):
-    _fields_ = [("perm", _vp), ("chunk", _i32), ("gref", _i32), ("nplanned", _i64)]
+class Batch(C.Structure):
+    _fields_ = [("workspace", _vp), ("workspace_bytes", C.c_size_t), ("facets_per_pack", _i32),
+                ("stripes_per_item", _i32), ("ctas_per_sm", _i32), ("flags", _i32)]
 
 
 class Pol(C.Structure):
@@ -101,13 +104,14 @@ SIGNATURES = {
     "ddfg_bda_mode1_count": (C.c_int, [_vp, _vp, _vp, _i32, _i32, _vp, _f64, _f64, _f64, _f64, _vp, _vp, _vp]),
     "ddfg_bda_mode1_write": (C.c_int, [_vp, _vp, _vp, _i32, _i32, _vp, _f64, _f64, _f64, _f64, _vp, _vp, _vp, _vp,
                                        _vp]),
-    "ddfg_sort_plan_workspace_size": (C.c_size_t, [_i64]),
-    "ddfg_sort_plan_build": (C.c_int, [C.POINTER(VisSet), C.POINTER(Facet), C.POINTER(SortPlan), _vp, C.c_size_t,
-                                       _vp]),
-    "ddfg_grid_sorted": (C.c_int, [C.POINTER(VisSet), C.POINTER(Jones), C.POINTER(Pol), C.POINTER(Facet), C.c_int,
-                                   C.c_int, C.POINTER(SortPlan), C.c_int, C.c_int, _vp]),
-    "ddfg_degrid_sorted": (C.c_int, [C.POINTER(VisSet), C.POINTER(Jones), C.POINTER(Pol), C.POINTER(Facet),
-                                     C.c_int, C.POINTER(SortPlan), C.c_int, _vp]),
+    "ddfg_batch_workspace_size": (C.c_size_t, []),
+    "ddfg_grid_batched": (C.c_int, [C.POINTER(VisSet), C.POINTER(Jones), C.POINTER(Pol), C.POINTER(Facet), C.c_int,
+                                    C.c_int, C.POINTER(Batch), _vp]),
+    "ddfg_degrid_batched": (C.c_int, [C.POINTER(VisSet), C.POINTER(Jones), C.POINTER(Pol), C.POINTER(Facet),
+                                      C.c_int, C.POINTER(Batch), _vp]),
+    "ddfg_block_geometry": (C.c_int, [C.POINTER(VisSet), C.POINTER(Facet), C.c_int, _vp, _vp]),
+    "ddfg_check_large_blocks_workspace_size": (C.c_size_t, [_i64]),
+    "ddfg_check_large_blocks": (C.c_int, [C.POINTER(VisSet), _vp, C.c_size_t, _vp]),
     "ddfg_fft_plan_create": (C.c_int, [_i32, _i32, C.POINTER(_vp)]),
     "ddfg_fft_plan_destroy": (C.c_int, [_vp]),
     "ddfg_grid_to_image": (C.c_int, [_vp, _vp, _f64, _vp, _vp]),

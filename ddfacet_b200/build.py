@@ -21,7 +21,7 @@ LIBDIR = os.path.join(HERE, "_lib")
 LIB = os.path.join(LIBDIR, "libddfg.so")
 INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 
-SOURCES = ["ddfg_abi.cu", "ddfg_plan.cu", "ddfg_grid.cu", "ddfg_degrid.cu", "ddfg_adjoint.cu", "ddfg_sorted.cu",
+SOURCES = ["ddfg_abi.cu", "ddfg_plan.cu", "ddfg_grid.cu", "ddfg_degrid.cu", "ddfg_adjoint.cu", "ddfg_geom.cu",
            "ddfg_fft.cu", "ddfg_weights.cu", "ddfg_bdamap.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

@@ -9,6 +9,9 @@
 #include <stdio.h>
 #include <string.h>
 
+#include <mutex>
+#include <unordered_map>
+
 #include "ddfg_common.cuh"
 #include "ddfg_internal.h"
 
@@ -185,7 +188,60 @@ int ddfg_num_ctas(int ctas_per_sm) {
   return cached_sms * ctas_per_sm;
 }
 
-extern "C" int ddfg_version(void) { return 1; }
+namespace {
+struct PrepKey {
+  const void *kernel;
+  int device, threads;
+  size_t smem;
+  bool operator==(const PrepKey &o) const {
+    return kernel == o.kernel && device == o.device && threads == o.threads && smem == o.smem;
+  }
+};
+struct PrepHash {
+  size_t operator()(const PrepKey &k) const {
+    return std::hash<const void *>()(k.kernel) ^ (std::hash<size_t>()(k.smem) * 31u) ^
+           (size_t)(k.device * 1315423911u) ^ (size_t)k.threads;
+  }
+};
+std::mutex g_prep_mutex;
+std::unordered_map<PrepKey, int, PrepHash> g_prep;
+// Dynamic shared-memory limit set so far per (kernel, device): it only ever grows, since a
+// launch needing more than the kernel's current limit fails.
+std::unordered_map<PrepKey, size_t, PrepHash> g_smem_limit;
+}  // namespace
+
+int ddfg_kernel_prepare(const void *kernel, int threads, size_t smem, int *per_sm) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return ddfg_set_error(DDFG_ECUDA, "kernel prepare: %s", cudaGetErrorString(e));
+  const PrepKey key{kernel, dev, threads, smem};
+  {
+    std::lock_guard<std::mutex> lock(g_prep_mutex);
+    auto it = g_prep.find(key);
+    if (it != g_prep.end()) {
+      *per_sm = it->second;
+      return DDFG_OK;
+    }
+  }
+  std::lock_guard<std::mutex> lock(g_prep_mutex);
+  const PrepKey kkey{kernel, dev, 0, 0};
+  size_t &limit = g_smem_limit[kkey];
+  if (smem > 48 * 1024 && smem > limit) {
+    e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess)
+      return ddfg_set_error(DDFG_ECUDA, "kernel prepare: %zu bytes of shared memory: %s", smem, cudaGetErrorString(e));
+    limit = smem;
+  }
+  int n = 0;
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kernel, threads, smem);
+  if (e != cudaSuccess) return ddfg_set_error(DDFG_ECUDA, "kernel prepare: %s", cudaGetErrorString(e));
+  if (n < 1) return ddfg_set_error(DDFG_ESIZE, "kernel prepare: %zu bytes of shared memory do not fit an SM", smem);
+  g_prep[key] = n;
+  *per_sm = n;
+  return DDFG_OK;
+}
+
+extern "C" int ddfg_version(void) { return 2; }
 
 extern "C" int ddfg_last_error(char *buf, int len) {
   if (!buf || len <= 0) return (int)strlen(g_err);
@@ -224,46 +280,7 @@ int degrid_checks(const ddfg_vis *vs, const ddfg_jones *js, const ddfg_pol *pol,
                             pol->npol);
   return DDFG_OK;
 }
-int max_sup(const ddfg_facet *facets, int n) {
-  int m = 1;
-  for (int i = 0; i < n; ++i) m = facets[i].max_support > m ? facets[i].max_support : m;
-  return m;
-}
-int plan_checks(const ddfg_sort_plan *plan, const ddfg_vis *vs) {
-  if (!plan || !plan->perm) return ddfg_set_error(DDFG_EINVAL, "sorted: null plan");
-  if (plan->gref <= 0 || plan->nplanned < 0) return ddfg_set_error(DDFG_EINVAL, "sorted: plan not built");
-  if (plan->nplanned > vs->nblocks) return ddfg_set_error(DDFG_EINVAL, "sorted: plan covers more blocks than the map has");
-  return DDFG_OK;
-}
 }  // namespace
-
-extern "C" int ddfg_grid_sorted(const ddfg_vis *vs, const ddfg_jones *js, const ddfg_pol *pol, const ddfg_facet *facets,
-                                int nfacets, int dopsf, const ddfg_sort_plan *plan, int compensated,
-                                int facets_per_launch, void *stream) {
-  g_err[0] = 0;
-  int policy = -1;
-  int rc = grid_checks(vs, js, pol, facets, nfacets, &policy);
-  if (rc) return rc;
-  rc = plan_checks(plan, vs);
-  if (rc) return rc;
-  if (nfacets == 0 || vs->nblocks == 0) return DDFG_OK;
-  return ddfg_launch_grid_sorted(vs, js, facets, nfacets, policy, pol->npol, dopsf, plan, compensated,
-                                 max_sup(facets, nfacets), facets_per_launch, (cudaStream_t)stream);
-}
-
-extern "C" int ddfg_degrid_sorted(const ddfg_vis *vs, const ddfg_jones *js, const ddfg_pol *pol,
-                                  const ddfg_facet *facets, int nfacets, const ddfg_sort_plan *plan,
-                                  int facets_per_launch, void *stream) {
-  g_err[0] = 0;
-  int policy = -1;
-  int rc = degrid_checks(vs, js, pol, facets, nfacets, &policy);
-  if (rc) return rc;
-  rc = plan_checks(plan, vs);
-  if (rc) return rc;
-  if (nfacets == 0 || vs->nblocks == 0) return DDFG_OK;
-  return ddfg_launch_degrid_sorted(vs, js, facets, nfacets, policy, pol->npol, plan, max_sup(facets, nfacets),
-                                   facets_per_launch, (cudaStream_t)stream);
-}
 
 extern "C" int ddfg_grid(const ddfg_vis *vs, const ddfg_jones *js, const ddfg_pol *pol, const ddfg_facet *facets,
                          int nfacets, int dopsf, void *stream) {
@@ -272,7 +289,51 @@ extern "C" int ddfg_grid(const ddfg_vis *vs, const ddfg_jones *js, const ddfg_po
   int rc = grid_checks(vs, js, pol, facets, nfacets, &policy);
   if (rc) return rc;
   if (nfacets == 0 || vs->nblocks == 0) return DDFG_OK;
-  return ddfg_launch_grid(vs, js, facets, nfacets, policy, pol->npol, dopsf, ddfg_num_ctas(4), (cudaStream_t)stream);
+  return ddfg_launch_grid(vs, js, facets, nfacets, policy, pol->npol, dopsf, nullptr, (cudaStream_t)stream);
+}
+
+extern "C" size_t ddfg_batch_workspace_size(void) {
+  return sizeof(unsigned long long) * (size_t)(kGridCounters + kDegridCounters);
+}
+
+namespace {
+int batch_checks(const ddfg_batch *batch, const char *who) {
+  if (!batch) return ddfg_set_error(DDFG_EINVAL, "%s: null batch", who);
+  if (batch->facets_per_pack < 0 || batch->stripes_per_item < 0 || batch->ctas_per_sm < 0)
+    return ddfg_set_error(DDFG_EINVAL, "%s: negative batch parameter", who);
+  if (!(batch->flags & 1)) {
+    if (!batch->workspace || batch->workspace_bytes < ddfg_batch_workspace_size())
+      return ddfg_set_error(DDFG_ESIZE, "%s: workspace %zu < %zu bytes", who, batch->workspace_bytes,
+                            ddfg_batch_workspace_size());
+    if ((uintptr_t)batch->workspace & 7) return ddfg_set_error(DDFG_EINVAL, "%s: workspace not 8-byte aligned", who);
+  }
+  return DDFG_OK;
+}
+}  // namespace
+
+extern "C" int ddfg_grid_batched(const ddfg_vis *vs, const ddfg_jones *js, const ddfg_pol *pol,
+                                 const ddfg_facet *facets, int nfacets, int dopsf, const ddfg_batch *batch,
+                                 void *stream) {
+  g_err[0] = 0;
+  int policy = -1;
+  int rc = grid_checks(vs, js, pol, facets, nfacets, &policy);
+  if (rc) return rc;
+  rc = batch_checks(batch, "grid_batched");
+  if (rc) return rc;
+  if (nfacets == 0 || vs->nblocks == 0) return DDFG_OK;
+  return ddfg_launch_grid(vs, js, facets, nfacets, policy, pol->npol, dopsf, batch, (cudaStream_t)stream);
+}
+
+extern "C" int ddfg_degrid_batched(const ddfg_vis *vs, const ddfg_jones *js, const ddfg_pol *pol,
+                                   const ddfg_facet *facets, int nfacets, const ddfg_batch *batch, void *stream) {
+  g_err[0] = 0;
+  int policy = -1;
+  int rc = degrid_checks(vs, js, pol, facets, nfacets, &policy);
+  if (rc) return rc;
+  rc = batch_checks(batch, "degrid_batched");
+  if (rc) return rc;
+  if (nfacets == 0 || vs->nblocks == 0) return DDFG_OK;
+  return ddfg_launch_degrid(vs, js, facets, nfacets, policy, pol->npol, batch, (cudaStream_t)stream);
 }
 
 extern "C" int ddfg_degrid(const ddfg_vis *vs, const ddfg_jones *js, const ddfg_pol *pol, const ddfg_facet *facets,
@@ -282,7 +343,7 @@ extern "C" int ddfg_degrid(const ddfg_vis *vs, const ddfg_jones *js, const ddfg_
   int rc = degrid_checks(vs, js, pol, facets, nfacets, &policy);
   if (rc) return rc;
   if (nfacets == 0 || vs->nblocks == 0) return DDFG_OK;
-  return ddfg_launch_degrid(vs, js, facets, nfacets, policy, pol->npol, ddfg_num_ctas(4), (cudaStream_t)stream);
+  return ddfg_launch_degrid(vs, js, facets, nfacets, policy, pol->npol, nullptr, (cudaStream_t)stream);
 }
 
 extern "C" int ddfg_degrid_adjoint(const ddfg_vis *vs, const ddfg_jones *js, const ddfg_pol *pol,

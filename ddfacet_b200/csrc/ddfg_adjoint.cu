@@ -440,9 +440,11 @@ int ddfg_launch_degrid_adjoint(const ddfg_vis *vs, const ddfg_jones *js, const d
   for (int i = 0; i < nfacets; ++i) max_support = max(max_support, facets[i].max_support);
   const int slots = tap_slots(max_support);
   const size_t smem = sizeof(ddfg_facet) * DDFG_FACETS_PER_LAUNCH + sizeof(double) * DDFG_FACETS_PER_LAUNCH;
-  for (int f0 = 0; f0 < nfacets; f0 += DDFG_FACETS_PER_LAUNCH) {
+  const int npacks = (nfacets + DDFG_FACETS_PER_LAUNCH - 1) / DDFG_FACETS_PER_LAUNCH;  // balanced packs
+  for (int ip = 0; ip < npacks; ++ip) {
+    const int f0 = (int)(((long long)ip * nfacets) / npacks);
     FacetPack pack;
-    pack.n = min(DDFG_FACETS_PER_LAUNCH, nfacets - f0);
+    pack.n = (int)(((long long)(ip + 1) * nfacets) / npacks) - f0;
     for (int i = 0; i < pack.n; ++i) pack.f[i] = facets[f0 + i];
 #define LAUNCH_A(NP, SL)                                                                      \
   do {                                                                                        \
@@ -475,18 +477,20 @@ int ddfg_launch_jones_grad(const ddfg_vis *vs, const ddfg_jones *js, const ddfg_
   const size_t smem = sizeof(ddfg_facet) * DDFG_FACETS_PER_LAUNCH + sizeof(double) * DDFG_FACETS_PER_LAUNCH +
                       (nvispol == 1 ? 8 * kPartialBytesPerWarp : 0);
   float2 *g = (float2 *)grad;
-  for (int f0 = 0; f0 < nfacets; f0 += DDFG_FACETS_PER_LAUNCH) {
+  int per_sm = 0;
+  const int npacks = (nfacets + DDFG_FACETS_PER_LAUNCH - 1) / DDFG_FACETS_PER_LAUNCH;  // balanced packs
+  for (int ip = 0; ip < npacks; ++ip) {
+    const int f0 = (int)(((long long)ip * nfacets) / npacks);
     FacetPackD pack;
-    pack.n = min(DDFG_FACETS_PER_LAUNCH, nfacets - f0);
+    pack.n = (int)(((long long)(ip + 1) * nfacets) / npacks) - f0;
     for (int i = 0; i < pack.n; ++i) pack.f[i] = facets[f0 + i];
 #define LAUNCH_J(NP, SL)                                                                                   \
   do {                                                                                                     \
     if (vs->single_vis_blocks) {                                                                           \
-      cudaFuncSetAttribute(jones_grad_kernel<NP, SL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem); \
+      ddfg_kernel_prepare((const void *)jones_grad_kernel<NP, SL>, 256, smem, &per_sm);                     \
       jones_grad_kernel<NP, SL><<<num_ctas, 256, smem, stream>>>(*vs, *js, pack, policy, g);                 \
     } else {                                                                                               \
-      cudaFuncSetAttribute(jones_grad_block_kernel<NP, SL>, cudaFuncAttributeMaxDynamicSharedMemorySize,     \
-                           (int)smem);                                                                     \
+      ddfg_kernel_prepare((const void *)jones_grad_block_kernel<NP, SL>, 256, smem, &per_sm);               \
       jones_grad_block_kernel<NP, SL><<<num_ctas, 256, smem, stream>>>(*vs, *js, pack, policy, g);           \
     }                                                                                                      \
   } while (0)

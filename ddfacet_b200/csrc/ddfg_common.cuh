@@ -441,16 +441,20 @@ struct LaneTaps {
   }
 };
 
+// dbg (nullable, [7]): the intermediate integers {iw, plane, locx, locy, offx, offy, k} as far as
+// they were formed (the rest untouched) -- ddfg_block_geometry reports them; the kernels pass NULL.
 __device__ __forceinline__ bool block_geometry(const ddfg_facet &f, double umean, double vmean, double wmean,
-                                               double recip_wvl, BlockGeom &g) {
+                                               double recip_wvl, BlockGeom &g, int *dbg = nullptr) {
   const double nwd = (double)f.nw;
   // iwplane = lrint((Nw-1)*|W|*(RefWave*recipWvl)/wmax)
   const double t0 = dmul(nwd - 1.0, fabs(wmean));
   const double t1 = dmul(f.ref_wave, recip_wvl);
   const long long iw = lrint_d(dmul(t0, t1) / f.wmax);
+  if (dbg) dbg[0] = iw > 0x7fffffffLL ? 0x7fffffff : (int)iw;
   if (iw >= f.nw) return false;
   if (iw < 0) return false;
   const int plane = (wmean > 0.) ? (int)iw : f.nw + (int)iw;
+  if (dbg) dbg[1] = plane;
   const int S = f.cf_support[plane];
   const int O = f.overs;
   const int nconv = S * O;
@@ -461,12 +465,21 @@ __device__ __forceinline__ bool block_geometry(const ddfg_facet &f, double umean
   const double posx = dadd(dmul(dmul(scx, umean), recip_wvl), (double)(f.nx / 2));
   const double posy = dadd(dmul(dmul(scy, vmean), recip_wvl), (double)(f.ny / 2));
   const long long lx = lrint_d(posx), ly = lrint_d(posy);
+  if (dbg) {
+    dbg[2] = (int)lx;
+    dbg[3] = (int)ly;
+  }
   if (lx - sup < 0 || lx + sup >= f.nx || ly - sup < 0 || ly + sup >= f.ny) return false;
   const int offx = (int)lrint_d(dmul(dsub((double)lx, posx), (double)O)) + (nconv - 1) / 2;
   const int offy = (int)lrint_d(dmul(dsub((double)ly, posy), (double)O)) + (nconv - 1) / 2;
   const int io = offy - sup * O;
   const int jo = offx - sup * O;
   const int k = io * O + jo;
+  if (dbg) {
+    dbg[4] = offx;
+    dbg[5] = offy;
+    dbg[6] = k;
+  }
   // A position exactly half-way between cells makes the reference read the neighbouring
   // sub-kernel; past either end of the plane it would read outside it, so skip those.
   if (k < 0 || k >= O * O) return false;

@@ -39,7 +39,7 @@ __device__ __forceinline__ void degrid_block_header(const ddfg_vis &vs, int64_t 
 
 // Footprint of block b on facet f; false when the reference skips it.
 __device__ __forceinline__ bool degrid_block_geom(const ddfg_vis &vs, const ddfg_facet &f, const DegridBlock &d,
-                                                  BlockGeom &g) {
+                                                  BlockGeom &g, int *dbg = nullptr) {
   if (d.ch1 <= d.ch0 || d.nrows <= 0) return false;
   if (d.gridchan < 0 || d.gridchan >= f.nband) return false;
   double um = 0., vm = 0., wm = 0.;
@@ -56,7 +56,7 @@ __device__ __forceinline__ bool degrid_block_geom(const ddfg_vis &vs, const ddfg
     wm = wm / dn;
   }
   const double rw = (d.ch1 - d.ch0 == 1 && vs.recip_wvl) ? vs.recip_wvl[d.ch0] : d.freqmean / kC;
-  return block_geometry(f, um, vm, wm, rw, g);
+  return block_geometry(f, um, vm, wm, rw, g, dbg);
 }
 
 // The block's Stokes -> correlation prediction with the per-block Jones (BDAJones), smearing

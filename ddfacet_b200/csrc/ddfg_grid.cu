@@ -1,154 +1,49 @@
 // BDA W-projection gridder for B200 (sm_100a).
 //
-// Restates DDFacet's gridder<> (DDFacet/Gridder/gridder.h:78-377) as a warp-cooperative kernel:
+// Restates DDFacet's gridder<> (DDFacet/Gridder/gridder.h:78-377) as persistent, queue-driven,
+// facet-inner kernels (ddfg_queue.cuh):
 //
 //  * one lane owns one BDA block (a baseline, rows r in R, channels [c0, c1)) and walks its
 //    visibilities exactly like the reference's hot loop 1 (gridder.h:182-301): first-corr flag,
 //    facet phasor exp(i nu angle) with an FP64 argument, per-antenna Jones J_p^H V J_q,
 //    weights, smearing factor, and the block means of (u + w Cu, v + w Cv, w, nu) in FP64 in
 //    the reference's summation order (so the integer grid indices agree bit-for-bit);
-//  * the block's Stokes value and footprint are then broadcast to the whole warp, whose 32
-//    lanes lay the S x S convolution taps (hot loop 2, gridder.h:353-375) onto the facet grid
-//    with vector complex atomics, consecutive lanes on consecutive cells of a CF row;
-//  * per-band weight sums and the Jones normalisation sums are reduced in shared memory and
-//    flushed once per CTA and facet.
+//  * the warp applies every facet of its pack to its stripe of 32 blocks in turn: the block's
+//    facet-independent inputs come from DRAM once per pack, the facet-dependent record (position,
+//    Jones, phasor, Stokes) is formed per facet, and the 32 lanes lay each record's S x S taps
+//    (hot loop 2, gridder.h:353-375) onto the facet grid with vector atomics (scatter_q: runs of
+//    records on the same cells merged in registers; TwoSum-compensated when the facet has a
+//    grid_lo buffer);
+//  * per-band weight sums and the Jones normalisation sums are reduced per warp into shared
+//    accumulators of the pack's facets and flushed when the CTA moves to another pack.
 //
-// One launch takes up to DDFG_FACETS_PER_LAUNCH facet descriptors as a kernel parameter; the
-// CTAs walk the facets one after the other, each over the whole block list, so the working set
-// in L2 is one facet's grid and CF tables at a time.
+// Single-visibility maps (every block one row and one channel) load the visibility's inputs once
+// per stripe (load_single); averaged blocks are walked per facet (their rows stay L1/L2-hot), and
+// blocks of the optional large-block list are walked by a whole warp each.
 #include <cuda_runtime.h>
 
 #include "ddfg_common.cuh"
 #include "ddfg_gridblock.cuh"
 #include "ddfg_internal.h"
-#include "ddfg_taps.cuh"
+#include "ddfg_queue.cuh"
 
 namespace ddfg {
 
-template <int NPOL, int SLOTS, bool SINGLE>
-__global__ void __launch_bounds__(256) grid_kernel(const ddfg_vis vs, const ddfg_jones js, const FacetPack pack,
-                                                   const GridParams gp) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  ddfg_facet *sf = (ddfg_facet *)smem_raw;
-  double *s_acc = (double *)(sf + pack.n);
-  stage_facets(pack, sf);
-  const int lane = threadIdx.x & 31;
-  const int warp = threadIdx.x >> 5;
-  const int nwarps = blockDim.x >> 5;
-  const int64_t nstripes = (vs.nblocks + 31) / 32;
-
-  for (int fi = 0; fi < pack.n; ++fi) {
-    __syncthreads();
-    const ddfg_facet &f = sf[fi];
-    const int npol_used = min(gp.nvispol, f.npol);
-    const int nsw = f.nband * f.npol;
-    double *s_sumwt = s_acc;                  // [nband][npol]
-    double *s_sumj = s_acc + nsw;             // [2][nband]
-    double *s_chan = s_sumj + 2 * f.nband;    // [2][nchan]
-    const int nacc = nsw + 2 * f.nband + 2 * vs.nchan;
-    for (int i = threadIdx.x; i < nacc; i += blockDim.x) s_acc[i] = 0.;
-    __syncthreads();
-
-    const double n0m1 = sqrt(1. - f.l0 * f.l0 - f.m0 * f.m0) - 1.;
-    JonesCache jc;
-    LaneTaps<SLOTS> lt;
-    lt.reset();
-
-    for (int64_t s = (int64_t)blockIdx.x * nwarps + warp; s < nstripes; s += (int64_t)gridDim.x * nwarps) {
-      const int64_t b = s * 32 + lane;
-      GridRecord<NPOL> rec;
-      rec.valid = false;
-      if (b < vs.nblocks) {
-        if (SINGLE) grid_single_record<NPOL>(vs, js, f, gp, b, n0m1, rec);
-        else grid_block_record<NPOL>(vs, js, f, gp, b, n0m1, rec, jc);
-      }
-
-      warp_add_block_sums<NPOL, SINGLE>(vs, js, f, gp, b, rec, npol_used, s_sumwt, s_sumj, s_chan, jc);
-
-      scatter_records<NPOL, SLOTS>(rec, f, npol_used, lt, lane);
-    }
-    __syncthreads();
-    // Flush this CTA's sums for facet fi.
-    for (int i = threadIdx.x; i < nsw; i += blockDim.x)
-      if (f.sumwt && s_sumwt[i] != 0.) atomicAdd(&f.sumwt[i], s_sumwt[i]);
-    if (js.mode != 0) {
-      for (int i = threadIdx.x; i < 2 * f.nband; i += blockDim.x)
-        if (f.sumjones && s_sumj[i] != 0.) atomicAdd(&f.sumjones[i], s_sumj[i]);
-      for (int i = threadIdx.x; i < 2 * vs.nchan; i += blockDim.x)
-        if (f.sumjones_chan && s_chan[i] != 0.) atomicAdd(&f.sumjones_chan[i], s_chan[i]);
-    }
-    __syncthreads();
+// The warp's records onto facet f: through the warp's tile when there is one and the records
+// qualify (one Stokes plane), else directly.
+template <int NPOL, int SLOTS>
+__device__ __forceinline__ void scatter_any(const GridRecord<NPOL> &rec, const ddfg_facet &f, int npol_used,
+                                            LaneTaps<SLOTS> &lt, LaneTaps<SLOTS> &ltt, int lane, float2 *wtile) {
+  if constexpr (NPOL == 1) {
+    if (wtile && scatter_tile<SLOTS>(rec, f, ltt, lane, wtile)) return;
   }
+  scatter_q<NPOL, SLOTS>(rec, f, npol_used, lt, lane);
 }
 
-// Averaged BDA blocks, facet-inner: each warp walks its 32 blocks for every facet of the launch
-// in turn (grid_block_record resets its Jones cache per block, so the order is free), so a
-// block's rows, visibilities, flags and weights are read from DRAM once per launch and from L1
-// for the other facets; per-facet shared accumulators hold the weight and Jones sums.  The block
-// walk needs ~170 registers: CTAs of 128 threads, three per SM (12 warps; 256-thread CTAs at the
-// unconstrained 212 registers fit once, 8 warps).
-template <int NPOL, int SLOTS>
-__global__ void __launch_bounds__(128, 3) grid_block_fi_kernel(const ddfg_vis vs, const ddfg_jones js,
-                                                            const FacetPack pack, const GridParams gp,
-                                                            int acc_stride) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  ddfg_facet *sf = (ddfg_facet *)smem_raw;
-  double *s_n0m1 = (double *)(sf + DDFG_FACETS_PER_LAUNCH);
-  double *s_acc = s_n0m1 + DDFG_FACETS_PER_LAUNCH;
-  stage_facets(pack, sf);
-  for (int i = threadIdx.x; i < pack.n * acc_stride; i += blockDim.x) s_acc[i] = 0.;
-  __syncthreads();
-  if (threadIdx.x < pack.n) {
-    const ddfg_facet &f = sf[threadIdx.x];
-    s_n0m1[threadIdx.x] = sqrt(1. - f.l0 * f.l0 - f.m0 * f.m0) - 1.;
-  }
-  __syncthreads();
-  const int lane = threadIdx.x & 31;
-  const int warp = threadIdx.x >> 5;
-  const int nwarps = blockDim.x >> 5;
-  const int64_t nstripes = (vs.nblocks + 31) / 32;
-  JonesCache jc;
-  LaneTaps<SLOTS> lt;
-  lt.reset();
-  for (int64_t s = (int64_t)blockIdx.x * nwarps + warp; s < nstripes; s += (int64_t)gridDim.x * nwarps) {
-    const int64_t b = s * 32 + lane;
-    // blocks of the large-block list are left to the second loop
-    const bool mine = b < vs.nblocks && !(vs.nlarge > 0 && block_nvis(vs, b) > vs.large_min_vis);
-    for (int fi = 0; fi < pack.n; ++fi) {
-      const ddfg_facet &f = sf[fi];
-      const int npol_used = min(gp.nvispol, f.npol);
-      double *a = s_acc + (size_t)fi * acc_stride;
-      GridRecord<NPOL> rec;
-      rec.valid = false;
-      if (mine) grid_block_record<NPOL>(vs, js, f, gp, b, s_n0m1[fi], rec, jc);
-      warp_add_block_sums<NPOL, false>(vs, js, f, gp, b, rec, npol_used, a, a + f.nband * f.npol,
-                                       a + f.nband * f.npol + 2 * f.nband, jc);
-      scatter_records<NPOL, SLOTS>(rec, f, npol_used, lt, lane);
-    }
-  }
-  // Large blocks, one warp each: lane 0 walks the FP64 means in the reference's order, the warp
-  // the rest (grid_block_record_warp); lane 0 holds the record the warp then lays down.
-  for (int64_t t = (int64_t)blockIdx.x * nwarps + warp; t < vs.nlarge; t += (int64_t)gridDim.x * nwarps) {
-    const int64_t bl = vs.large_blocks[t];
-    if (vs.sparsification && !vs.sparsification[bl]) continue;
-    for (int fi = 0; fi < pack.n; ++fi) {
-      const ddfg_facet &f = sf[fi];
-      const int npol_used = min(gp.nvispol, f.npol);
-      double *a = s_acc + (size_t)fi * acc_stride;
-      double *a_chan = a + f.nband * f.npol + 2 * f.nband;
-      BlockMeans bm{};
-      if (lane == 0) bm = grid_block_means(vs, f, bl);
-      GridRecord<NPOL> rec;
-      rec.valid = false;
-      rec.single_chan = true;
-      grid_block_record_warp<NPOL>(vs, js, f, gp, bl, bm, s_n0m1[fi], 0, lane, npol_used, a_chan, rec);
-      warp_add_block_sums<NPOL, false>(vs, js, f, gp, bl, rec, npol_used, a, a + f.nband * f.npol, a_chan, jc,
-                                       !rec.single_chan);
-      scatter_records<NPOL, SLOTS>(rec, f, npol_used, lt, lane);
-    }
-  }
-  __syncthreads();
-  for (int fi = 0; fi < pack.n; ++fi) {
+// Adds the CTA's shared sums of the pack's npk facets to their float64 outputs.
+__device__ __forceinline__ void flush_grid_sums(const ddfg_facet *sf, int npk, const double *s_acc, int acc_stride,
+                                                const ddfg_jones &js, int nchan) {
+  for (int fi = 0; fi < npk; ++fi) {
     const ddfg_facet &f = sf[fi];
     const double *a = s_acc + (size_t)fi * acc_stride;
     const int nsw = f.nband * f.npol;
@@ -157,72 +52,167 @@ __global__ void __launch_bounds__(128, 3) grid_block_fi_kernel(const ddfg_vis vs
     if (js.mode != 0) {
       for (int i = threadIdx.x; i < 2 * f.nband; i += blockDim.x)
         if (f.sumjones && a[nsw + i] != 0.) atomicAdd(&f.sumjones[i], a[nsw + i]);
-      for (int i = threadIdx.x; i < 2 * vs.nchan; i += blockDim.x)
-        if (f.sumjones_chan && a[nsw + 2 * f.nband + i] != 0.) atomicAdd(&f.sumjones_chan[i], a[nsw + 2 * f.nband + i]);
+      for (int i = threadIdx.x; i < 2 * nchan; i += blockDim.x)
+        if (f.sumjones_chan && a[nsw + 2 * f.nband + i] != 0.)
+          atomicAdd(&f.sumjones_chan[i], a[nsw + 2 * f.nband + i]);
     }
   }
 }
 
-// Single-visibility blocks, facet-inner: each warp loads its 32 visibilities' facet-independent
-// inputs (map entries, uvw, flags, weights, visibilities, Jones indices) once and grids them onto
-// every facet of the launch in turn, instead of re-reading them once per facet.  Per-facet weight
-// and Jones sums have their own shared-memory accumulators (acc_stride doubles each).
+// Moves the CTA to pack `pack` if it is not there yet: flushes the old pack's sums, stages the new
+// pack's descriptors and zeroes its accumulators.  All threads call it, after queue_next.
+__device__ __forceinline__ void enter_pack(const FacetTable &tab, const Sched &sc, const ddfg_jones &js, int nchan,
+                                           int pack, int &cur, int &npk, ddfg_facet *sf, double *s_n0m1,
+                                           double *s_acc) {
+  if (pack == cur) return;
+  if (cur >= 0) flush_grid_sums(sf, npk, s_acc, sc.acc_stride, js, nchan);
+  __syncthreads();
+  npk = stage_pack(tab, sc, pack, sf, s_n0m1);
+  for (int i = threadIdx.x; i < npk * sc.acc_stride; i += blockDim.x) s_acc[i] = 0.;
+  cur = pack;
+  __syncthreads();
+}
+
+// Single-visibility blocks: each warp loads its 32 visibilities' facet-independent inputs (map
+// entries, uvw, flags, weights, visibilities, Jones indices) once and grids them onto every facet
+// of the pack in turn.
 template <int NPOL, int SLOTS>
-__global__ void __launch_bounds__(256) grid_single_fi_kernel(const ddfg_vis vs, const ddfg_jones js,
-                                                             const FacetPack pack, const GridParams gp,
-                                                             int acc_stride) {
+__global__ void __launch_bounds__(256) grid_single_q(const ddfg_vis vs, const ddfg_jones js,
+                                                     const __grid_constant__ FacetTable tab, const GridParams gp,
+                                                     const Sched sc) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  ddfg_facet *sf = (ddfg_facet *)smem_raw;
-  double *s_n0m1 = (double *)(sf + DDFG_FACETS_PER_LAUNCH);
-  double *s_acc = s_n0m1 + DDFG_FACETS_PER_LAUNCH;
-  stage_facets(pack, sf);
-  for (int i = threadIdx.x; i < pack.n * acc_stride; i += blockDim.x) s_acc[i] = 0.;
-  __syncthreads();
-  if (threadIdx.x < pack.n) {
-    const ddfg_facet &f = sf[threadIdx.x];
-    s_n0m1[threadIdx.x] = sqrt(1. - f.l0 * f.l0 - f.m0 * f.m0) - 1.;
-  }
-  __syncthreads();
+  float2 *wtile = (float2 *)smem_raw + (threadIdx.x >> 5) * kTileCells;  // [warps][kTileCells] if sc.tiles
+  ddfg_facet *sf = (ddfg_facet *)(smem_raw + (sc.tiles ? (blockDim.x >> 5) * kTileCells * sizeof(float2) : 0));
+  double *s_n0m1 = (double *)(sf + sc.max_pack);
+  double *s_acc = s_n0m1 + sc.max_pack;
+  __shared__ QueueSmem q;
   const int lane = threadIdx.x & 31;
-  const int warp = threadIdx.x >> 5;
-  const int nwarps = blockDim.x >> 5;
-  const int64_t nstripes = (vs.nblocks + 31) / 32;
   JonesCache jc;  // not used by single-visibility blocks
-  LaneTaps<SLOTS> lt;
+  LaneTaps<SLOTS> lt, ltt;
   lt.reset();
-
-  for (int64_t s = (int64_t)blockIdx.x * nwarps + warp; s < nstripes; s += (int64_t)gridDim.x * nwarps) {
-    const int64_t b = s * 32 + lane;
-    SingleIn in;
-    in.valid = false;
-    if (b < vs.nblocks) load_single(vs, js, gp, b, in);
-    if (!__any_sync(0xffffffffu, in.valid)) continue;
-    for (int fi = 0; fi < pack.n; ++fi) {
-      const ddfg_facet &f = sf[fi];
-      const int npol_used = min(gp.nvispol, f.npol);
-      double *a = s_acc + (size_t)fi * acc_stride;
-      double *a_sumwt = a;                      // [nband][npol]
-      double *a_sumj = a + f.nband * f.npol;    // [2][nband]
-      double *a_chan = a_sumj + 2 * f.nband;    // [2][nchan]
-      GridRecord<NPOL> rec;
-      grid_single_facet<NPOL>(in, vs, js, f, gp, s_n0m1[fi], rec);
-      warp_add_block_sums<NPOL, true>(vs, js, f, gp, b, rec, npol_used, a_sumwt, a_sumj, a_chan, jc);
-      scatter_records<NPOL, SLOTS>(rec, f, npol_used, lt, lane);
+  ltt.reset();
+  long long static_next = blockIdx.x;
+  int cur = -1, npk = 0;
+  for (;;) {
+    const long long item = queue_next(sc, &q, static_next);
+    if (item >= sc.nitems) break;
+    const int pack = (int)(item / sc.items_per_pack);
+    const long long s0 = (item - (long long)pack * sc.items_per_pack - sc.large_items) * sc.spi;
+    enter_pack(tab, sc, js, vs.nchan, pack, cur, npk, sf, s_n0m1, s_acc);
+    const int ns = (int)min(sc.spi, sc.nstripes - s0);
+    for (int k; (k = warp_take(&q, ns, lane)) >= 0;) {
+      const int64_t b = (s0 + k) * 32 + lane;
+      SingleIn in;
+      in.valid = false;
+      if (b < vs.nblocks) load_single(vs, js, gp, b, in);
+      if (!__any_sync(0xffffffffu, in.valid)) continue;
+      for (int fi = 0; fi < npk; ++fi) {
+        const ddfg_facet &f = sf[fi];
+        const int npol_used = min(gp.nvispol, f.npol);
+        double *a = s_acc + (size_t)fi * sc.acc_stride;
+        double *a_sumj = a + f.nband * f.npol;
+        GridRecord<NPOL> rec;
+        grid_single_facet<NPOL>(in, vs, js, f, gp, s_n0m1[fi], rec);
+        warp_add_block_sums<NPOL, true>(vs, js, f, gp, b, rec, npol_used, a, a_sumj, a_sumj + 2 * f.nband, jc);
+        scatter_any<NPOL, SLOTS>(rec, f, npol_used, lt, ltt, lane, sc.tiles ? wtile : nullptr);
+      }
     }
   }
-  __syncthreads();
-  // Flush this CTA's sums for every facet of the launch.
-  for (int fi = 0; fi < pack.n; ++fi) {
-    const ddfg_facet &f = sf[fi];
-    const double *a = s_acc + (size_t)fi * acc_stride;
-    const int nsw = f.nband * f.npol;
-    for (int i = threadIdx.x; i < nsw; i += blockDim.x)
-      if (f.sumwt && a[i] != 0.) atomicAdd(&f.sumwt[i], a[i]);
-    if (js.mode != 0) {
-      for (int i = threadIdx.x; i < 2 * f.nband; i += blockDim.x)
-        if (f.sumjones && a[nsw + i] != 0.) atomicAdd(&f.sumjones[i], a[nsw + i]);
-      for (int i = threadIdx.x; i < 2 * vs.nchan; i += blockDim.x)
-        if (f.sumjones_chan && a[nsw + 2 * f.nband + i] != 0.) atomicAdd(&f.sumjones_chan[i], a[nsw + 2 * f.nband + i]);
+  if (cur >= 0) flush_grid_sums(sf, npk, s_acc, sc.acc_stride, js, vs.nchan);
+}
+
+// Averaged BDA blocks: each warp walks its 32 blocks for every facet of the pack in turn
+// (grid_block_record resets its Jones cache per block, so the order is free); a block's rows,
+// visibilities, flags and weights come from DRAM once per pack and from L1/L2 for the other
+// facets.  Large-block items give each listed block to one warp: lane 0 walks the FP64 means in
+// the reference's order, the warp the rest (grid_block_record_warp).  The block walk needs ~170
+// registers: CTAs of 128 threads, three per SM.
+template <int NPOL, int SLOTS>
+__global__ void __launch_bounds__(128, 3) grid_block_q(const ddfg_vis vs, const ddfg_jones js,
+                                                       const __grid_constant__ FacetTable tab, const GridParams gp,
+                                                       const Sched sc) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  float2 *wtile = (float2 *)smem_raw + (threadIdx.x >> 5) * kTileCells;  // [warps][kTileCells] if sc.tiles
+  ddfg_facet *sf = (ddfg_facet *)(smem_raw + (sc.tiles ? (blockDim.x >> 5) * kTileCells * sizeof(float2) : 0));
+  double *s_n0m1 = (double *)(sf + sc.max_pack);
+  double *s_acc = s_n0m1 + sc.max_pack;
+  __shared__ QueueSmem q;
+  const int lane = threadIdx.x & 31;
+  JonesCache jc;
+  LaneTaps<SLOTS> lt, ltt;
+  lt.reset();
+  ltt.reset();
+  long long static_next = blockIdx.x;
+  int cur = -1, npk = 0;
+  for (;;) {
+    const long long item = queue_next(sc, &q, static_next);
+    if (item >= sc.nitems) break;
+    const int pack = (int)(item / sc.items_per_pack);
+    const long long r = item - (long long)pack * sc.items_per_pack;
+    enter_pack(tab, sc, js, vs.nchan, pack, cur, npk, sf, s_n0m1, s_acc);
+    if (r < sc.large_items) {
+      const long long t0 = r * sc.large_per_item;
+      const int nt = (int)min((long long)sc.large_per_item, vs.nlarge - t0);
+      for (int k; (k = warp_take(&q, nt, lane)) >= 0;) {
+        const int64_t bl = vs.large_blocks[t0 + k];
+        // entries that are out of range or not above the threshold belong to the stripes
+        if (bl < 0 || bl >= vs.nblocks || block_nvis(vs, bl) <= vs.large_min_vis) continue;
+        if (vs.sparsification && !vs.sparsification[bl]) continue;
+        for (int fi = 0; fi < npk; ++fi) {
+          const ddfg_facet &f = sf[fi];
+          const int npol_used = min(gp.nvispol, f.npol);
+          double *a = s_acc + (size_t)fi * sc.acc_stride;
+          double *a_chan = a + f.nband * f.npol + 2 * f.nband;
+          BlockMeans bm{};
+          if (lane == 0) bm = grid_block_means(vs, f, bl);
+          GridRecord<NPOL> rec;
+          rec.valid = false;
+          rec.single_chan = true;
+          grid_block_record_warp<NPOL>(vs, js, f, gp, bl, bm, s_n0m1[fi], 0, lane, npol_used, a_chan, rec);
+          warp_add_block_sums<NPOL, false>(vs, js, f, gp, bl, rec, npol_used, a, a + f.nband * f.npol, a_chan, jc,
+                                           !rec.single_chan);
+          scatter_any<NPOL, SLOTS>(rec, f, npol_used, lt, ltt, lane, sc.tiles ? wtile : nullptr);
+        }
+      }
+      continue;
+    }
+    const long long s0 = (r - sc.large_items) * sc.spi;
+    const int ns = (int)min(sc.spi, sc.nstripes - s0);
+    for (int k; (k = warp_take(&q, ns, lane)) >= 0;) {
+      const int64_t b = (s0 + k) * 32 + lane;
+      // blocks above the large-block threshold are the large items' work
+      const bool mine = b < vs.nblocks && !(vs.nlarge > 0 && block_nvis(vs, b) > vs.large_min_vis);
+      for (int fi = 0; fi < npk; ++fi) {
+        const ddfg_facet &f = sf[fi];
+        const int npol_used = min(gp.nvispol, f.npol);
+        double *a = s_acc + (size_t)fi * sc.acc_stride;
+        GridRecord<NPOL> rec;
+        rec.valid = false;
+        if (mine) grid_block_record<NPOL>(vs, js, f, gp, b, s_n0m1[fi], rec, jc);
+        warp_add_block_sums<NPOL, false>(vs, js, f, gp, b, rec, npol_used, a, a + f.nband * f.npol,
+                                         a + f.nband * f.npol + 2 * f.nband, jc);
+        scatter_any<NPOL, SLOTS>(rec, f, npol_used, lt, ltt, lane, sc.tiles ? wtile : nullptr);
+      }
+    }
+  }
+  if (cur >= 0) flush_grid_sums(sf, npk, s_acc, sc.acc_stride, js, vs.nchan);
+}
+
+// grid += grid_lo; grid_lo = 0, for every facet of the table that has a compensation buffer.
+__global__ void fold_lo_kernel(const __grid_constant__ FacetTable tab, int nfacets) {
+  const int fi = blockIdx.y;
+  if (fi >= nfacets) return;
+  const ddfg_facet &f = tab.f[fi];
+  if (!f.grid_lo) return;
+  float2 *hi = (float2 *)f.grid;
+  float2 *lo = (float2 *)f.grid_lo;
+  const int64_t n = (int64_t)f.nband * f.npol * f.ny * f.nx;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const float2 l = lo[i];
+    if (l.x != 0.f || l.y != 0.f) {
+      const float2 h = hi[i];
+      hi[i] = make_float2(h.x + l.x, h.y + l.y);
+      lo[i] = czero();
     }
   }
 }
@@ -231,99 +221,116 @@ __global__ void __launch_bounds__(256) grid_single_fi_kernel(const ddfg_vis vs, 
 
 using namespace ddfg;
 
+namespace {
+
+template <int NP, int SL>
+int launch_grid_table(const ddfg_vis *vs, const ddfg_jones *js, const FacetTable &tab, const GridParams &gp,
+                      Sched sc, const ddfg_batch *batch, cudaStream_t stream) {
+  const bool single = vs->single_vis_blocks != 0;
+  const int threads = single ? 256 : 128;
+  const size_t smem = (sc.tiles ? (size_t)(threads / 32) * kTileCells * sizeof(float2) : 0) +
+                      (sizeof(ddfg_facet) + sizeof(double)) * (size_t)sc.max_pack +
+                      sizeof(double) * (size_t)sc.max_pack * (size_t)sc.acc_stride;
+  const void *kern = single ? (const void *)grid_single_q<NP, SL> : (const void *)grid_block_q<NP, SL>;
+  int per_sm = 0;
+  int rc = ddfg_kernel_prepare(kern, threads, smem, &per_sm);
+  if (rc) return rc;
+  if (batch && batch->ctas_per_sm > 0) per_sm = min(per_sm, (int)batch->ctas_per_sm);
+  const int ctas = ddfg_num_ctas(per_sm);
+  if (single) grid_single_q<NP, SL><<<ctas, threads, smem, stream>>>(*vs, *js, tab, gp, sc);
+  else grid_block_q<NP, SL><<<ctas, threads, smem, stream>>>(*vs, *js, tab, gp, sc);
+  const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return ddfg_set_error(DDFG_ECUDA, "grid launch: %s", cudaGetErrorString(e));
+  return DDFG_OK;
+}
+
+}  // namespace
+
 int ddfg_launch_grid(const ddfg_vis *vs, const ddfg_jones *js, const ddfg_facet *facets, int nfacets, int policy,
-                     int nvispol, int dopsf, int num_ctas, cudaStream_t stream) {
-  int max_support = 1;
-  for (int i = 0; i < nfacets; ++i) max_support = max(max_support, facets[i].max_support);
+                     int nvispol, int dopsf, const ddfg_batch *batch, cudaStream_t stream) {
+  int max_support = 1, max_band = 1;
+  bool any_lo = false;
+  for (int i = 0; i < nfacets; ++i) {
+    max_support = max(max_support, facets[i].max_support);
+    max_band = max(max_band, facets[i].nband * (facets[i].npol + 2));
+    any_lo = any_lo || facets[i].grid_lo != nullptr;
+  }
   const int slots = tap_slots(max_support);
   GridParams gp;
   gp.policy = policy;
   gp.nvispol = nvispol;
   gp.dopsf = dopsf;
   gp.freq_mean0 = vs->freq_mean;
-  int max_band = 1;
-  for (int i = 0; i < nfacets; ++i) max_band = max(max_band, facets[i].nband * (facets[i].npol + 2));
-  const size_t smem = sizeof(ddfg_facet) * DDFG_FACETS_PER_LAUNCH + sizeof(double) * ((size_t)max_band + 2 * (size_t)vs->nchan);
-  if (smem > 160 * 1024) return ddfg_set_error(DDFG_ESIZE, "grid: too many bands/channels for the shared accumulators");
-  // Facet-inner single-visibility kernel when every facet's accumulators fit in shared memory.
   const int acc_stride = max_band + 2 * vs->nchan;
-  const size_t smem_fi = sizeof(ddfg_facet) * DDFG_FACETS_PER_LAUNCH + sizeof(double) * DDFG_FACETS_PER_LAUNCH +
-                         sizeof(double) * (size_t)DDFG_FACETS_PER_LAUNCH * (size_t)acc_stride;
-  const bool facet_inner = vs->single_vis_blocks && smem_fi <= 64 * 1024;
-  const bool block_fi = !vs->single_vis_blocks && smem_fi <= 64 * 1024;
-  for (int f0 = 0; f0 < nfacets; f0 += DDFG_FACETS_PER_LAUNCH) {
-    FacetPack pack;
-    pack.n = min(DDFG_FACETS_PER_LAUNCH, nfacets - f0);
-    for (int i = 0; i < pack.n; ++i) pack.f[i] = facets[f0 + i];
-    const int npol = nvispol;
-    cudaError_t e;
-    if (block_fi) {
-#define LAUNCH_B1(NP, SL)                                                                                          \
-  do {                                                                                                             \
-    if (smem_fi > 48 * 1024)                                                                                       \
-      cudaFuncSetAttribute(grid_block_fi_kernel<NP, SL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_fi); \
-    grid_block_fi_kernel<NP, SL><<<ddfg_one_wave(grid_block_fi_kernel<NP, SL>, 128, smem_fi), 128, smem_fi, stream>>>( \
-        *vs, *js, pack, gp, acc_stride);                                                                           \
-  } while (0)
-#define LAUNCH_B_NP(SL)              \
-  switch (npol) {                    \
-    case 1: LAUNCH_B1(1, SL); break; \
-    case 2: LAUNCH_B1(2, SL); break; \
-    case 3: LAUNCH_B1(3, SL); break; \
-    default: LAUNCH_B1(4, SL); break; \
+  const size_t per_facet_smem = sizeof(ddfg_facet) + sizeof(double) + sizeof(double) * (size_t)acc_stride;
+  // Shared memory per CTA: two 256-thread CTAs (single-visibility maps) or three 128-thread CTAs
+  // (averaged blocks) per SM, each with the warps' grid tiles (one Stokes plane) and the shared
+  // accumulators of a pack.
+  const bool single = vs->single_vis_blocks != 0;
+  const size_t budget = single ? 110 * 1024 : 74 * 1024;
+  const size_t tile_bytes = (size_t)(single ? 8 : 4) * kTileCells * sizeof(float2);
+  int tiles = (nvispol == 1 && !(batch && (batch->flags & 2))) ? 1 : 0;
+  if (tiles && budget < tile_bytes + per_facet_smem) tiles = 0;
+  const int max_fit = (int)((budget - (tiles ? tile_bytes : 0)) / per_facet_smem);
+  if (max_fit < 1) return ddfg_set_error(DDFG_ESIZE, "grid: too many bands/channels for the shared accumulators");
+  int want = (batch && batch->facets_per_pack > 0) ? batch->facets_per_pack : 16;
+  want = max(1, min(want, max_fit));
+  unsigned long long *counters = nullptr;
+  const int ngroups = (nfacets + DDFG_TABLE_FACETS - 1) / DDFG_TABLE_FACETS;
+  if (batch && !(batch->flags & 1)) {
+    counters = (unsigned long long *)batch->workspace;
+    const cudaError_t e = cudaMemsetAsync(counters, 0, sizeof(unsigned long long) * ngroups, stream);
+    if (e != cudaSuccess) return ddfg_set_error(DDFG_ECUDA, "grid: %s", cudaGetErrorString(e));
   }
-      if (slots == 2) { LAUNCH_B_NP(2) } else if (slots == 4) { LAUNCH_B_NP(4) } else { LAUNCH_B_NP(8) }
-#undef LAUNCH_B_NP
-#undef LAUNCH_B1
-      e = cudaGetLastError();
-      if (e != cudaSuccess) return ddfg_set_error(DDFG_ECUDA, "grid launch: %s", cudaGetErrorString(e));
-      continue;
+  const long long nstripes = (vs->nblocks + 31) / 32;
+  const int nlarge = vs->single_vis_blocks ? 0 : (int)(vs->nlarge < (1LL << 30) ? vs->nlarge : (1LL << 30));
+  FacetTable tab_tl;  // host staging of the parameter table (copied into the launch)
+  for (int g = 0; g < ngroups; ++g) {
+    const int f0 = (int)(((long long)g * nfacets) / ngroups), f1 = (int)(((long long)(g + 1) * nfacets) / ngroups);
+    const int n = f1 - f0;
+    for (int i = 0; i < n; ++i) tab_tl.f[i] = facets[f0 + i];
+    Sched sc;
+    sc.nfacets = n;
+    sc.npacks = (n + want - 1) / want;
+    sc.max_pack = (n + sc.npacks - 1) / sc.npacks;
+    sc.acc_stride = acc_stride;
+    sc.tiles = tiles;
+    sc.nstripes = nstripes;
+    // default: items of 16-256 stripes, about four per resident CTA and pack
+    const long long spi = (batch && batch->stripes_per_item > 0) ? batch->stripes_per_item
+                                                                 : max(16LL, min(256LL, nstripes / 1184));
+    sc.spi = max(1LL, spi);
+    sc.stripe_items = (nstripes + sc.spi - 1) / sc.spi;
+    sc.large_per_item = vs->single_vis_blocks ? 8 : 4;
+    sc.large_items = (nlarge + sc.large_per_item - 1) / sc.large_per_item;
+    sc.items_per_pack = sc.large_items + sc.stripe_items;
+    sc.nitems = sc.items_per_pack * sc.npacks;
+    sc.counter = counters ? counters + g : nullptr;
+    int rc;
+#define LG(NP, SL) rc = launch_grid_table<NP, SL>(vs, js, tab_tl, gp, sc, batch, stream)
+#define LG_NP(SL)                \
+  switch (nvispol) {             \
+    case 1: LG(1, SL); break;    \
+    case 2: LG(2, SL); break;    \
+    case 3: LG(3, SL); break;    \
+    default: LG(4, SL); break;   \
+  }
+    if (slots == 2) { LG_NP(2) } else if (slots == 4) { LG_NP(4) } else { LG_NP(8) }
+#undef LG_NP
+#undef LG
+    if (rc) return rc;
+    if (any_lo) {
+      int64_t cells = 0;
+      for (int i = 0; i < n; ++i)
+        {
+          const int64_t c = (int64_t)tab_tl.f[i].nband * tab_tl.f[i].npol * tab_tl.f[i].ny * tab_tl.f[i].nx;
+          if (c > cells) cells = c;
+        }
+      const int bx = (int)((cells + 255) / 256 < 1024 ? (cells + 255) / 256 : 1024);
+      fold_lo_kernel<<<dim3(bx, n), 256, 0, stream>>>(tab_tl, n);
+      const cudaError_t e = cudaGetLastError();
+      if (e != cudaSuccess) return ddfg_set_error(DDFG_ECUDA, "grid fold: %s", cudaGetErrorString(e));
     }
-    if (facet_inner) {
-#define LAUNCH_F1(NP, SL)                                                                                          \
-  do {                                                                                                             \
-    if (smem_fi > 48 * 1024)                                                                                       \
-      cudaFuncSetAttribute(grid_single_fi_kernel<NP, SL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_fi); \
-    grid_single_fi_kernel<NP, SL><<<num_ctas, 256, smem_fi, stream>>>(*vs, *js, pack, gp, acc_stride);             \
-  } while (0)
-#define LAUNCH_F_NP(SL)              \
-  switch (npol) {                    \
-    case 1: LAUNCH_F1(1, SL); break; \
-    case 2: LAUNCH_F1(2, SL); break; \
-    case 3: LAUNCH_F1(3, SL); break; \
-    default: LAUNCH_F1(4, SL); break; \
-  }
-      if (slots == 2) { LAUNCH_F_NP(2) } else if (slots == 4) { LAUNCH_F_NP(4) } else { LAUNCH_F_NP(8) }
-#undef LAUNCH_F_NP
-#undef LAUNCH_F1
-      e = cudaGetLastError();
-      if (e != cudaSuccess) return ddfg_set_error(DDFG_ECUDA, "grid launch: %s", cudaGetErrorString(e));
-      continue;
-    }
-#define LAUNCH_G1(NP, SL, SG)                                                                                 \
-  do {                                                                                                        \
-    if (smem > 48 * 1024)                                                                                     \
-      cudaFuncSetAttribute(grid_kernel<NP, SL, SG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);  \
-    grid_kernel<NP, SL, SG><<<num_ctas, 256, smem, stream>>>(*vs, *js, pack, gp);                             \
-  } while (0)
-#define LAUNCH_G(NP, SL)                                 \
-  do {                                                   \
-    if (vs->single_vis_blocks) LAUNCH_G1(NP, SL, true);  \
-    else LAUNCH_G1(NP, SL, false);                       \
-  } while (0)
-#define LAUNCH_G_NP(SL)            \
-  switch (npol) {                  \
-    case 1: LAUNCH_G(1, SL); break; \
-    case 2: LAUNCH_G(2, SL); break; \
-    case 3: LAUNCH_G(3, SL); break; \
-    default: LAUNCH_G(4, SL); break; \
-  }
-    if (slots == 2) { LAUNCH_G_NP(2) } else if (slots == 4) { LAUNCH_G_NP(4) } else { LAUNCH_G_NP(8) }
-#undef LAUNCH_G_NP
-#undef LAUNCH_G
-#undef LAUNCH_G1
-    e = cudaGetLastError();
-    if (e != cudaSuccess) return ddfg_set_error(DDFG_ECUDA, "grid launch: %s", cudaGetErrorString(e));
   }
   return DDFG_OK;
 }

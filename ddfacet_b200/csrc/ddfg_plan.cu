@@ -100,9 +100,9 @@ extern "C" int ddfg_bda_plan(const int32_t *bda_map, int64_t bda_len, int64_t nb
 // allocation after start-up, or a caller that has no workspace to offer at that point.  For
 // them ddfg_bda_plan_noalloc keeps its scratch (the prefix-sum temporaries and the check's error
 // word) in the fixed array below, which every GPU that loads the library holds until the
-// process exits.  The array's address is looked up once per device, with that device current,
-// the first time the entry point runs on it; that first call should therefore come before any
-// stream capture.  All calls on a device share the array: two calls that overlap on the GPU
+// process exits.  The array's address is looked up with the device current on every call made
+// outside stream capture; a call made during capture reuses the last address, so the first call
+// on a device should come before any stream capture.  All calls on a device share the array: two calls that overlap on the GPU
 // (different streams, or different host threads) race, so callers serialise them.
 // ------------------------------------------------------------------------------------------
 #include <mutex>
@@ -116,14 +116,19 @@ constexpr int kMaxDevices = 64;
 std::mutex g_noalloc_mutex;
 void *g_noalloc_addr[kMaxDevices] = {nullptr};
 
-// Device address of the scratch array on the current device (looked up once per device).
-int noalloc_scratch(void **out) {
+// Device address of the scratch array on the current device.  It is looked up again on every
+// call made outside stream capture (so a context re-created after cudaDeviceReset gets its own
+// address), and the last address is kept for calls made while the stream is being captured.
+int noalloc_scratch(void **out, cudaStream_t stream) {
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return ddfg_set_error(DDFG_ECUDA, "bda_plan_noalloc: %s", cudaGetErrorString(e));
   if (dev < 0 || dev >= kMaxDevices) return ddfg_set_error(DDFG_ESIZE, "bda_plan_noalloc: device %d >= %d", dev, kMaxDevices);
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  e = cudaStreamIsCapturing(stream, &cap);
+  if (e != cudaSuccess) return ddfg_set_error(DDFG_ECUDA, "bda_plan_noalloc: %s", cudaGetErrorString(e));
   std::lock_guard<std::mutex> lock(g_noalloc_mutex);
-  if (!g_noalloc_addr[dev]) {
+  if (!g_noalloc_addr[dev] || cap == cudaStreamCaptureStatusNone) {
     void *p = nullptr;
     e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
     if (e != cudaSuccess || !p)
@@ -146,7 +151,7 @@ extern "C" int ddfg_bda_plan_noalloc(const int32_t *bda_map, int64_t bda_len, in
     return ddfg_set_error(DDFG_EINVAL, "bda_plan_noalloc: null pointer or bad length");
   if (bda_len < 2 + nblocks) return ddfg_set_error(DDFG_EMAP, "bda_plan_noalloc: map shorter than its block table");
   void *scratch = nullptr;
-  int rc = noalloc_scratch(&scratch);
+  int rc = noalloc_scratch(&scratch, stream);
   if (rc) return rc;
   // Layout: [prefix-sum temporaries ... | error word in the last 256 bytes]
   size_t tmp_bytes = 0;

@@ -180,7 +180,22 @@ class VisData:
         st = self.block_start
         nv = sizes * (self.bda_map[st + 1].to(torch.int64) - self.bda_map[st].to(torch.int64))
         idx = torch.nonzero(nv > int(min_vis)).flatten().contiguous()
-        return replace(self, large_blocks=idx if idx.numel() else None, large_min_vis=int(min_vis))
+        out = replace(self, large_blocks=idx if idx.numel() else None, large_min_vis=int(min_vis))
+        if out.vis.is_cuda:
+            out.check_large_blocks()
+        return out
+
+    def check_large_blocks(self, stream=None):
+        """Validates the large-block list on the device (ddfg_check_large_blocks): raises if an entry
+        is not a block index, is listed twice or is not above the threshold, or if a block above
+        the threshold is missing."""
+        if self.large_blocks is None or self.large_blocks.numel() == 0:
+            return
+        lib = _abi.lib()
+        ws = torch.empty(int(lib.ddfg_check_large_blocks_workspace_size(self.nblocks)), dtype=torch.uint8,
+                         device=self.vis.device)
+        vss = self.struct()
+        _abi.check(lib.ddfg_check_large_blocks(C.byref(vss), ws.data_ptr(), ws.numel(), _stream_ptr(stream)))
 
     def struct(self) -> _abi.VisSet:
         s = _abi.VisSet()
@@ -257,6 +272,15 @@ class FacetGrid:
     sumwt: Optional[torch.Tensor] = None        # float64 [nband, npol]
     sumjones: Optional[torch.Tensor] = None     # float64 [2, nband]
     sumjones_chan: Optional[torch.Tensor] = None  # float64 [2, nchan]
+    grid_lo: Optional[torch.Tensor] = None      # complex64 like grid: compensated gridding (all zero)
+
+    def with_compensation(self) -> "FacetGrid":
+        """This facet with a compensation buffer (ddfg_facet.grid_lo): gridding into it adds the
+        float32 rounding error of every grid addition to the buffer and folds it into the grid at
+        the end of each call, so each call adds the correctly rounded sum of its contributions."""
+        if self.grid_lo is None:
+            self.grid_lo = torch.zeros_like(self.grid)
+        return self
 
     def struct(self, degrid=False) -> _abi.Facet:
         s = _abi.Facet()
@@ -276,6 +300,7 @@ class FacetGrid:
         s.sumwt = _ptr(self.sumwt)
         s.sumjones = _ptr(self.sumjones)
         s.sumjones_chan = _ptr(self.sumjones_chan)
+        s.grid_lo = None if degrid else _ptr(self.grid_lo)
         return s
 
 
@@ -334,71 +359,83 @@ def make_pol(corr_ids, stokes_ids) -> _abi.Pol:
     return p
 
 
-def grid(vs: VisData, facets: List[FacetGrid], pol: _abi.Pol, jones: Optional[JonesData] = None, dopsf=False,
-         stream=None):
-    """Grid ``vs`` onto every facet (ddfg_grid)."""
-    lib = _abi.lib()
-    arr = (_abi.Facet * max(1, len(facets)))(*[f.struct(degrid=False) for f in facets])
-    js = (jones or JonesData()).struct()
-    vss = vs.struct()
-    _abi.check(lib.ddfg_grid(C.byref(vss), C.byref(js), C.byref(pol), arr, len(facets), int(bool(dopsf)),
-                             _stream_ptr(stream)))
-
-
-def degrid(vs: VisData, facets: List[FacetGrid], pol: _abi.Pol, jones: Optional[JonesData] = None, stream=None):
-    """Subtract every facet's prediction from ``vs.vis`` (ddfg_degrid)."""
-    lib = _abi.lib()
-    arr = (_abi.Facet * max(1, len(facets)))(*[f.struct(degrid=True) for f in facets])
-    js = (jones or JonesData()).struct()
-    vss = vs.struct()
-    _abi.check(lib.ddfg_degrid(C.byref(vss), C.byref(js), C.byref(pol), arr, len(facets), _stream_ptr(stream)))
-
-
 @dataclass
-class SortPlan:
-    """Work list of the batched kernels (ddfg_sort_plan_build): block indices sorted by (band,
-    W-plane support, grid row, grid column) on the largest facet grid."""
-    perm: torch.Tensor
-    st: _abi.SortPlan
+class Batch:
+    """Scheduling of the batched (persistent, queue-driven) calls and their workspace
+    (ddfg_batch): facets per pack, stripes per queue item, resident CTAs per SM (0 = library
+    default); ``static`` replaces the queue by a fixed item order and ``no_tiles`` turns off the
+    warps' grid tiles (both for measurements)."""
+    workspace: torch.Tensor
+    facets_per_pack: int = 0
+    stripes_per_item: int = 0
+    ctas_per_sm: int = 0
+    static: bool = False
+    no_tiles: bool = False
 
     @classmethod
-    def build(cls, vs: VisData, facets: List[FacetGrid], chunk=1024, stream=None):
+    def create(cls, device=None, **kw) -> "Batch":
         lib = _abi.lib()
-        ref = max(facets, key=lambda f: f.grid.shape[-1])
-        nb = vs.nblocks
-        perm = torch.empty(max(nb, 1), dtype=torch.int64, device=vs.vis.device)
-        p = _abi.SortPlan()
-        p.perm = perm.data_ptr()
-        p.chunk = int(chunk)
-        ws = torch.empty(int(lib.ddfg_sort_plan_workspace_size(nb)), dtype=torch.uint8, device=vs.vis.device)
-        vss = vs.struct()
-        fs = ref.struct()
-        _abi.check(lib.ddfg_sort_plan_build(C.byref(vss), C.byref(fs), C.byref(p), ws.data_ptr(), ws.numel(),
-                                            _stream_ptr(stream)))
-        return cls(perm, p)
+        ws = torch.zeros(int(lib.ddfg_batch_workspace_size()), dtype=torch.uint8, device=_dev(device))
+        return cls(workspace=ws, **kw)
+
+    def struct(self) -> _abi.Batch:
+        b = _abi.Batch()
+        b.workspace = self.workspace.data_ptr()
+        b.workspace_bytes = self.workspace.numel()
+        b.facets_per_pack = int(self.facets_per_pack)
+        b.stripes_per_item = int(self.stripes_per_item)
+        b.ctas_per_sm = int(self.ctas_per_sm)
+        b.flags = (1 if self.static else 0) | (2 if self.no_tiles else 0)
+        return b
+
+    def describe(self) -> dict:
+        return {"facets_per_pack": int(self.facets_per_pack), "stripes_per_item": int(self.stripes_per_item),
+                "ctas_per_sm": int(self.ctas_per_sm), "queue": not self.static, "tiles": not self.no_tiles}
 
 
-def grid_sorted(vs: VisData, facets: List[FacetGrid], pol: _abi.Pol, plan: SortPlan, jones: Optional[JonesData] = None,
-                dopsf=False, compensated=True, facets_per_launch=0, stream=None):
-    """Grid ``vs`` onto every facet through the sort plan (ddfg_grid_sorted)."""
+def grid(vs: VisData, facets: List[FacetGrid], pol: _abi.Pol, jones: Optional[JonesData] = None, dopsf=False,
+         stream=None, batch: Optional[Batch] = None):
+    """Grid ``vs`` onto every facet: ddfg_grid, or ddfg_grid_batched with a ``batch``."""
     lib = _abi.lib()
     arr = (_abi.Facet * max(1, len(facets)))(*[f.struct(degrid=False) for f in facets])
     js = (jones or JonesData()).struct()
     vss = vs.struct()
-    _abi.check(lib.ddfg_grid_sorted(C.byref(vss), C.byref(js), C.byref(pol), arr, len(facets), int(bool(dopsf)),
-                                    C.byref(plan.st), int(bool(compensated)), int(facets_per_launch),
-                                    _stream_ptr(stream)))
+    if batch is None:
+        _abi.check(lib.ddfg_grid(C.byref(vss), C.byref(js), C.byref(pol), arr, len(facets), int(bool(dopsf)),
+                                 _stream_ptr(stream)))
+    else:
+        bs = batch.struct()
+        _abi.check(lib.ddfg_grid_batched(C.byref(vss), C.byref(js), C.byref(pol), arr, len(facets),
+                                         int(bool(dopsf)), C.byref(bs), _stream_ptr(stream)))
 
 
-def degrid_sorted(vs: VisData, facets: List[FacetGrid], pol: _abi.Pol, plan: SortPlan,
-                  jones: Optional[JonesData] = None, facets_per_launch=0, stream=None):
-    """Subtract every facet's prediction from ``vs.vis`` through the sort plan (ddfg_degrid_sorted)."""
+def degrid(vs: VisData, facets: List[FacetGrid], pol: _abi.Pol, jones: Optional[JonesData] = None, stream=None,
+           batch: Optional[Batch] = None):
+    """Subtract every facet's prediction from ``vs.vis``: ddfg_degrid, or ddfg_degrid_batched with
+    a ``batch``."""
     lib = _abi.lib()
     arr = (_abi.Facet * max(1, len(facets)))(*[f.struct(degrid=True) for f in facets])
     js = (jones or JonesData()).struct()
     vss = vs.struct()
-    _abi.check(lib.ddfg_degrid_sorted(C.byref(vss), C.byref(js), C.byref(pol), arr, len(facets), C.byref(plan.st),
-                                      int(facets_per_launch), _stream_ptr(stream)))
+    if batch is None:
+        _abi.check(lib.ddfg_degrid(C.byref(vss), C.byref(js), C.byref(pol), arr, len(facets), _stream_ptr(stream)))
+    else:
+        bs = batch.struct()
+        _abi.check(lib.ddfg_degrid_batched(C.byref(vss), C.byref(js), C.byref(pol), arr, len(facets), C.byref(bs),
+                                           _stream_ptr(stream)))
+
+
+def block_geometry(vs: VisData, facet: FacetGrid, degrid=False, stream=None) -> torch.Tensor:
+    """int32 [nblocks, 8] = (status, iw, plane, locx, locy, offx, offy, k) of every block on
+    ``facet`` as the gridder (or, with ``degrid``, the degridder) computes them
+    (ddfg_block_geometry)."""
+    lib = _abi.lib()
+    out = torch.full((max(vs.nblocks, 1), 8), -1, dtype=torch.int32, device=vs.vis.device)
+    vss = vs.struct()
+    fs = facet.struct(degrid=degrid)
+    _abi.check(lib.ddfg_block_geometry(C.byref(vss), C.byref(fs), int(bool(degrid)), out.data_ptr(),
+                                       _stream_ptr(stream)))
+    return out[:vs.nblocks]
 
 
 def capture_graph(fn, warmup: int = 1):

@@ -37,8 +37,13 @@ extern "C" {
 
 /* Maximum number of facets one ddfg_grid / ddfg_degrid call may take. */
 #define DDFG_MAX_FACETS 1024
-/* Facets whose descriptors travel in one kernel launch (the rest go in further launches). */
+/* Facets whose descriptors travel in one kernel launch of the backward passes (the rest go in
+ * further launches of balanced size). */
 #define DDFG_FACETS_PER_LAUNCH 16
+/* Facets whose descriptors travel in one launch of ddfg_grid / ddfg_degrid and their batched
+ * variants (a __grid_constant__ kernel parameter table); a call with more facets makes further
+ * launches of balanced size. */
+#define DDFG_TABLE_FACETS 128
 
 /* One facet: its grid, geometry, W-projection tables and outputs.
  * Replaces the per-facet arguments of pyGridderWPol / pyDeGridderWPol
@@ -64,6 +69,14 @@ typedef struct ddfg_facet {
   double *sumwt;               /* [nband][npol]   (sumwt)                                 */
   double *sumjones;            /* [2][nband]      (LJones[17])                            */
   double *sumjones_chan;       /* [2][nchan]      (LJones[18])                            */
+  /* Compensated gridding (optional; NULL = plain float32 accumulation).  A complex64 buffer of
+   * the grid's shape, all zero on entry, that ddfg_grid / ddfg_grid_batched use for the rounding
+   * error of every grid addition (TwoSum of the value an atomic add returns and the addend); at the
+   * end of the call it is added into grid once and left all zero again.  The grid then holds the
+   * float32 rounding of the call's exact sum (plus its previous contents) instead of the sum of
+   * ~10^4-10^6 successively rounded additions per cell.  No counterpart in the reference, which adds
+   * its double products into the float grid (gridder.h:360-362). */
+  void *grid_lo;
 } ddfg_facet;
 
 /* The visibilities and everything indexed by row/channel (facet independent). */
@@ -128,15 +141,21 @@ typedef struct ddfg_pol {
   int32_t stokes_ids[4];
 } ddfg_pol;
 
-/* The work list of the batched kernels: blocks sorted by (grid band, support of the W plane,
- * grid row, grid column) of their mean position on a reference facet grid.  Consecutive blocks
- * then share grid cells, which the kernels exploit.  The caller owns perm. */
-typedef struct ddfg_sort_plan {
-  int64_t *perm;               /* [nblocks] block indices in sorted order                 */
-  int32_t chunk;               /* in: blocks per warp work item                           */
-  int32_t gref;                /* out: side of the reference facet grid                   */
-  int64_t nplanned;            /* out: blocks that can be gridded (sorted first)          */
-} ddfg_sort_plan;
+/* Scheduling of ddfg_grid_batched / ddfg_degrid_batched: one persistent launch per call (per
+ * DDFG_TABLE_FACETS facets) whose CTAs take work items from a queue in device memory.  An item
+ * is a run of stripes (32 consecutive blocks) of one facet pack; the warps of a CTA apply every
+ * facet of the pack to a stripe in turn (its inputs are read once per pack).  Items are ordered
+ * pack by pack, the large-block items of a pack first (the longest work starts first).  Zero
+ * fields take the library's defaults (or the autotuner's choice, ddfacet_b200.autotune). */
+typedef struct ddfg_batch {
+  void *workspace;             /* >= ddfg_batch_workspace_size() bytes of device scratch, 8-byte aligned */
+  size_t workspace_bytes;
+  int32_t facets_per_pack;     /* facets applied to a stripe before the next stripe (0: default) */
+  int32_t stripes_per_item;    /* stripes of one queue item (0: default)                   */
+  int32_t ctas_per_sm;         /* resident CTAs per SM of the persistent launch (0: occupancy) */
+  int32_t flags;               /* bit 0: static item order instead of the queue; bit 1: no warp
+                                  grid tiles (direct tap additions) -- both for measurements */
+} ddfg_batch;
 
 /* Library and device checks. */
 int ddfg_version(void);
@@ -249,36 +268,50 @@ int ddfg_bda_mode1_write(const double *uvw, const int32_t *rows, const int64_t *
  * reference.  Same inputs, outputs and checks as ddfg_bda_plan, but no workspace argument: its
  * scratch is a fixed 1 MiB array inside the library, held by every GPU that loads the library
  * until the process exits, so maps are limited to DDFG_BDA_PLAN_NOALLOC_MAX_BLOCKS blocks
- * (DDFG_ESIZE above that).  It allocates nothing.  Its first call on a device looks up that
- * array's device address (with the device current), so make that first call before any stream
- * capture.  Calls share the array: calls that overlap on the GPU race and must be serialised by
+ * (DDFG_ESIZE above that).  It allocates nothing.  Each call made outside stream capture looks
+ * up that array's device address (with the device current); a call made while the stream is
+ * being captured reuses the last address, so make the first call on a device before any stream
+ * capture (and, after a cudaDeviceReset, one more call outside capture).  Calls share the array: calls that overlap on the GPU race and must be serialised by
  * the caller. */
 int ddfg_bda_plan_noalloc(const int32_t *bda_map, int64_t bda_len, int64_t nblocks, int64_t nrow, int32_t nchan,
                           int64_t *block_start, void *stream, int32_t *single_out);
 
-/* Device scratch of ddfg_sort_plan_build (bytes). */
-size_t ddfg_sort_plan_workspace_size(int64_t nblocks);
+/* Bytes of device scratch ddfg_grid_batched / ddfg_degrid_batched need (the queue counters). */
+size_t ddfg_batch_workspace_size(void);
 
-/* Keys every block of vs by its band, W-plane support and grid cell on the reference facet ref,
- * and sorts the blocks (stable radix sort, so the order is deterministic).  A plan call: it
- * synchronises the stream.  The plan stays valid while the block map, uvw, frequencies and
- * channel map are unchanged; it does not depend on the visibilities, weights, flags or Jones. */
-int ddfg_sort_plan_build(const ddfg_vis *vs, const ddfg_facet *ref, ddfg_sort_plan *plan, void *workspace,
-                         size_t workspace_bytes, void *stream);
+/* ddfg_grid as one persistent, queue-driven launch per DDFG_TABLE_FACETS facets (see
+ * ddfg_batch): same inputs, outputs and checks.  The work queue balances uneven facets and
+ * blocks (averaged BDA blocks of very different sizes) across the GPU; every call first resets
+ * its counters (one cudaMemsetAsync), so the call can be captured in a CUDA graph.  Replaces the
+ * per-facet gridding jobs of ClassFacetMachine (ClassFacetMachine.py:1574-1592). */
+int ddfg_grid_batched(const ddfg_vis *vs, const ddfg_jones *js, const ddfg_pol *pol, const ddfg_facet *facets,
+                      int nfacets, int dopsf, const ddfg_batch *batch, void *stream);
 
-/* ddfg_grid over a sort plan (the batched gridder).  Each warp walks a chunk of consecutive
- * sorted blocks and keeps the footprint's tap sums in registers while the grid cell and support
- * stay the same, writing them to the grid once per run; compensated != 0 adds TwoSum error terms
- * to the register sums.  facets_per_launch (<= DDFG_FACETS_PER_LAUNCH, 0 = default) bounds the
- * facets whose grids are live in L2 at once.  Facets of one call must share nband and npol. */
-int ddfg_grid_sorted(const ddfg_vis *vs, const ddfg_jones *js, const ddfg_pol *pol, const ddfg_facet *facets,
-                     int nfacets, int dopsf, const ddfg_sort_plan *plan, int compensated, int facets_per_launch,
-                     void *stream);
+/* ddfg_degrid the same way (ClassFacetMachine.py:1912-1944).  With facets_per_pack >= nfacets
+ * every visibility is read and written once per call. */
+int ddfg_degrid_batched(const ddfg_vis *vs, const ddfg_jones *js, const ddfg_pol *pol, const ddfg_facet *facets,
+                        int nfacets, const ddfg_batch *batch, void *stream);
 
-/* ddfg_degrid over a sort plan (the batched degridder): each warp keeps the footprint's model
- * grid values in registers while consecutive blocks share the grid cell. */
-int ddfg_degrid_sorted(const ddfg_vis *vs, const ddfg_jones *js, const ddfg_pol *pol, const ddfg_facet *facets,
-                       int nfacets, const ddfg_sort_plan *plan, int facets_per_launch, void *stream);
+/* The integer footprint of every block on one facet, as the gridder (degrid_means 0) or the
+ * degridder (1) computes it (gridder.h:321-351, degridder.h:168-200): out int32 [nblocks][8] =
+ * {status, iw, plane, locx, locy, offx, offy, cf sub-kernel index} where iw is the w-plane
+ * index lrint((Nw-1)|W|RefWave nu/c/wmax), plane the CF table used (iw for W > 0, nw + iw for
+ * LcfsConj), (locx, locy) the centre cell and (offx, offy) the oversampling offsets; status 1 =
+ * gridded/degridded, 0 = skipped (no unflagged visibility, band outside the grid, w beyond
+ * wmax, support outside the grid), in which case the later fields are -1 from the first skipped
+ * step on.  Uses the kernels' own index code.  A check entry point: the reference exposes these
+ * indices only inside its loops. */
+int ddfg_block_geometry(const ddfg_vis *vs, const ddfg_facet *facet, int degrid_means, int32_t *out, void *stream);
+
+/* Bytes of device scratch ddfg_check_large_blocks needs. */
+size_t ddfg_check_large_blocks_workspace_size(int64_t nblocks);
+
+/* Checks vs->large_blocks: every entry a block index in [0, nblocks), listed once, and the list
+ * holds exactly the blocks of more than large_min_vis visibilities.  A plan call: it synchronises
+ * the stream and returns DDFG_EMAP for a bad list.  (The kernels also skip list entries that are
+ * out of range or not above the threshold, so a bad list cannot make them read out of bounds or
+ * grid a small block twice.) */
+int ddfg_check_large_blocks(const ddfg_vis *vs, void *workspace, size_t workspace_bytes, void *stream);
 
 /* ---- per-facet transforms and stitching --------------------------------------------- */
 

@@ -154,3 +154,24 @@ def degrid(model, vis0, uvw, freqs, chan_map, bda_map, wplanes, wconj, overs, re
     if rc:
         raise ValueError("unsupported correlation/Stokes combination")
     return v
+
+
+def block_indices(uvw, flags, freqs, chan_map, bda_map, wplanes, wconj, overs, ref_wave, wmax, incr, cu, cv, nband,
+                  npix, degrid=False):
+    """int32 [nblocks, 8] = (status, iw, plane, locx, locy, offx, offy, k) of every block, from the
+    gridder's (flag-aware) or the degridder's block means: the integer indices of gridder.h:321-351
+    restated in FP64 C, for a word-by-word comparison with ddfg_block_geometry."""
+    nrow, nchan, ncorr = flags.shape
+    cf, off, sup = _pack_cf(wplanes, wconj, overs, degrid=degrid)
+    bm = np.ascontiguousarray(bda_map, np.int32)
+    nb = int(np.uint32(bm[0])) + (int(bm[1]) << 32)
+    out = np.full((max(nb, 1), 8), -1, np.int32)
+    fl = np.ascontiguousarray(flags).view(np.uint8) if flags.dtype == bool else np.ascontiguousarray(flags, np.uint8)
+    arrs = [np.ascontiguousarray(uvw, np.float64), fl, np.ascontiguousarray(freqs, np.float64),
+            np.ascontiguousarray(chan_map, np.int32)]
+    f = lib().fp64_block_indices
+    f.restype = C.c_int
+    f(_p(arrs[0]), _p(arrs[1]), nchan, ncorr, _p(arrs[2]), _p(arrs[3]), _p(bm), _p(off), _p(sup), len(wplanes),
+      int(overs), C.c_double(ref_wave), C.c_double(wmax), int(npix), int(npix), int(nband), C.c_double(incr[0]),
+      C.c_double(incr[1]), C.c_double(cu), C.c_double(cv), int(bool(degrid)), _p(out))
+    return out[:nb]

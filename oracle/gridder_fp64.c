@@ -17,6 +17,9 @@
 #include <stdint.h>
 #include <stdlib.h>
 #include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
 
 typedef double complex dc;
 typedef float complex fc;
@@ -231,27 +234,103 @@ static int corr_degrid(int cs, const char *st, const dc *s, M *r) {
   return 0;
 }
 
-/* W plane, location and CF offset (gridder.h:321-351).  Returns 0 to skip. */
+/* W plane, location and CF offset (gridder.h:321-351).  Returns 0 to skip.  dbg (nullable, [7])
+ * receives {iw, plane, locx, locy, offx, offy, k} as far as they are formed. */
 static int geometry(double nw, int overs, double ref_wave, double wmax, const int64_t *cf_off, const int *cf_sup,
                     int nx, int ny, double incr_x, double incr_y, double U, double V, double W, double recip,
-                    int64_t *cfo, int *lx, int *ly, int *S) {
+                    int64_t *cfo, int *lx, int *ly, int *S, int *dbg) {
   long iw = lrint((nw - 1) * fabs(W) * (ref_wave * recip) / wmax);
+  if (dbg) dbg[0] = iw > 0x7fffffffL ? 0x7fffffff : (int)iw;
   if (iw >= (long)nw || iw < 0) return 0;
   int plane = (W > 0) ? (int)iw : (int)nw + (int)iw;
+  if (dbg) dbg[1] = plane;
   int s = cf_sup[plane], nconv = s * overs, sup = (s - 1) / 2;
   double posx = nx * incr_x * U * recip + (double)(nx / 2);
   double posy = nx * incr_y * V * recip + (double)(ny / 2);
   long locx = lrint(posx), locy = lrint(posy);
+  if (dbg) { dbg[2] = (int)locx; dbg[3] = (int)locy; }
   if (locx - sup < 0 || locx + sup >= nx || locy - sup < 0 || locy + sup >= ny) return 0;
   int offx = (int)(lrint((locx - posx) * overs) + (nconv - 1) / 2);
   int offy = (int)(lrint((locy - posy) * overs) + (nconv - 1) / 2);
   int k = (offy - sup * overs) * overs + (offx - sup * overs);
+  if (dbg) { dbg[4] = offx; dbg[5] = offy; dbg[6] = k; }
   if (k < 0 || k >= overs * overs) return 0;
   *cfo = cf_off[plane] + (int64_t)k * s * s;
   *lx = (int)locx;
   *ly = (int)locy;
   *S = s;
   return 1;
+}
+
+/* Word index of every block record of a packed map (the sequential walk of gridder.h:144-148). */
+static int64_t *block_starts(const int *bmap, size_t nb) {
+  int64_t *st = malloc(sizeof(int64_t) * (nb ? nb : 1));
+  int64_t w = 2 + (int64_t)nb;
+  for (size_t b = 0; b < nb; ++b) {
+    st[b] = w;
+    w += bmap[2 + b];
+  }
+  return st;
+}
+
+/* {status, iw, plane, locx, locy, offx, offy, k} of every block, from the gridder's block means
+ * (unflagged visibilities, gridder.h:272-289) or, with degrid_means, the degridder's (rows and
+ * channels, degridder.h:138-167): the integer indices the GPU's ddfg_block_geometry reports. */
+int fp64_block_indices(const double *uvw, const uint8_t *flags, int nchan, int ncorr, const double *freqs,
+                       const int *chan_map, const int *bmap, const int64_t *cf_off, const int *cf_sup, int nw,
+                       int overs, double ref_wave, double wmax, int nx, int ny, int nband, double incr_x,
+                       double incr_y, double cu, double cv, int degrid_means, int *out) {
+  size_t nb = (size_t)(uint32_t)bmap[0] + ((size_t)bmap[1] << 32);
+  int64_t *st = block_starts(bmap, nb);
+#pragma omp parallel for schedule(dynamic, 4096)
+  for (size_t b = 0; b < nb; ++b) {
+    const int *p = bmap + st[b];
+    int nr = bmap[2 + b] - 2, c0 = p[0], c1 = p[1];
+    const int *rows = p + 2;
+    int dbg[7] = {-1, -1, -1, -1, -1, -1, -1}, ok = 0;
+    int64_t cfo;
+    int lx, ly, S;
+    double um = 0, vmn = 0, wm = 0, fm = 0;
+    int gch = chan_map[c0 < nchan ? c0 : 0];
+    if (degrid_means) {
+      if (gch >= 0 && gch < nband && nr > 0 && c1 > c0) {
+        for (int c = c0; c < c1; ++c) fm += freqs[c];
+        if (c1 - c0 > 1) fm /= (c1 - c0);
+        for (int i = 0; i < nr; ++i) {
+          const double *u = uvw + 3 * (int64_t)rows[i];
+          um += u[0] + u[2] * cu;
+          vmn += u[1] + u[2] * cv;
+          wm += u[2];
+        }
+        if (nr > 1) { um /= nr; vmn /= nr; wm /= nr; }
+        ok = geometry(nw, overs, ref_wave, wmax, cf_off, cf_sup, nx, ny, incr_x, incr_y, um, vmn, wm, fm / C_LIGHT,
+                      &cfo, &lx, &ly, &S, dbg);
+      }
+    } else {
+      int n = 0;
+      for (int i = 0; i < nr; ++i) {
+        const double *u = uvw + 3 * (int64_t)rows[i];
+        for (int c = c0; c < c1; ++c) {
+          if (flags[((int64_t)rows[i] * nchan + c) * ncorr]) continue;
+          um += u[0] + u[2] * cu;
+          vmn += u[1] + u[2] * cv;
+          wm += u[2];
+          fm += freqs[c];
+          ++n;
+        }
+      }
+      if (n > 0 && gch >= 0 && gch < nband) {
+        if (n > 1) { um /= n; vmn /= n; wm /= n; fm /= n; }
+        ok = geometry(nw, overs, ref_wave, wmax, cf_off, cf_sup, nx, ny, incr_x, incr_y, um, vmn, wm, fm / C_LIGHT,
+                      &cfo, &lx, &ly, &S, dbg);
+      }
+    }
+    int *o = out + 8 * b;
+    o[0] = ok;
+    for (int i = 0; i < 7; ++i) o[1 + i] = dbg[i];
+  }
+  free(st);
+  return 0;
 }
 
 /* Returns 0, or -2 for an unsupported correlation/Stokes combination. */
@@ -270,12 +349,31 @@ int fp64_grid(dc *grid, int nband, int npol, int ny, int nx, const fc *vis, cons
   for (int c = 0; c < nchan; ++c) fm0 += freqs[c];
   fm0 /= nchan;
   size_t nb = (size_t)(uint32_t)bmap[0] + ((size_t)bmap[1] << 32);
-  const int *sizes = bmap + 2, *p = bmap + 2 + nb;
+  const int *sizes = bmap + 2;
+  int64_t *starts = block_starts(bmap, nb);
+  const size_t gcells = (size_t)nband * npol * nx * ny;
+  /* Large maps run on all host threads, each into its own complex128 grid and sums (added in
+   * thread order at the end); small ones on one thread. */
+  int nthr = 1;
+#ifdef _OPENMP
+  if (nb > 200000) nthr = omp_get_max_threads();
+#endif
+#pragma omp parallel num_threads(nthr)
+  {
+  int tid = 0;
+#ifdef _OPENMP
+  tid = omp_get_thread_num();
+#endif
+  dc *tgrid = tid == 0 ? grid : calloc(gcells, sizeof(dc));
+  double *tsumwt = calloc((size_t)nband * npol, sizeof(double));
+  double *tsj = calloc(2 * (size_t)nband, sizeof(double));
+  double *tsjc = calloc(2 * (size_t)nchan, sizeof(double));
   double *chj = calloc((size_t)nchan, sizeof(double)), *chq = calloc((size_t)nchan, sizeof(double));
+#pragma omp for schedule(dynamic, 2048)
   for (size_t b = 0; b < nb; ++b) {
+    const int *p = bmap + starts[b];
     int nr = sizes[b] - 2, c0 = p[0], c1 = p[1];
     const int *rows = p + 2;
-    p += sizes[b];
     if (sparsification && !sparsification[b]) continue;
     if (nr <= 0) continue;
     memset(chj, 0, sizeof(double) * nchan);
@@ -345,30 +443,49 @@ int fp64_grid(dc *grid, int nband, int npol, int ny, int nx, const fc *vis, cons
     int64_t cfo;
     int lx, ly, S;
     if (!geometry(nw, overs, ref_wave, wmax, cf_off, cf_sup, nx, ny, incr_x, incr_y, um, vmn, wm, fm / C_LIGHT, &cfo,
-                  &lx, &ly, &S))
+                  &lx, &ly, &S, NULL))
       continue;
     dc sv[4];
     stokes_grid(cs, st, acc, sv);
     int sup = (S - 1) / 2;
     for (int ip = 0; ip < nstokes; ++ip) {
       if (ip >= npol) continue;
-      dc *g = grid + ((size_t)gch * npol + ip) * (size_t)nx * ny;
+      dc *g = tgrid + ((size_t)gch * npol + ip) * (size_t)nx * ny;
       const fc *c = cf + cfo;
       for (int sy = -sup; sy <= sup; ++sy)
         for (int sx = -sup; sx <= sup; ++sx) g[(size_t)(ly + sy) * nx + lx + sx] += sv[ip] * (dc)(*c++);
-      sumwt[ip + gch * npol] += tw;
+      tsumwt[ip + gch * npol] += tw;
       if (js->mode) {
-        sumjones[gch] += sj;
-        sumjones[gch + nband] += sq;
+        tsj[gch] += sj;
+        tsj[gch + nband] += sq;
         for (int cc = c0; cc < c1; ++cc) {
-          sumjones_chan[cc] += chj[cc];
-          sumjones_chan[nchan + cc] += chq[cc];
+          tsjc[cc] += chj[cc];
+          tsjc[nchan + cc] += chq[cc];
         }
       }
     }
   }
+  /* thread order: deterministic for a given thread count */
+  for (int t = 0; t < nthr; ++t) {
+#pragma omp barrier
+    if (t == tid) {
+      if (tid != 0)
+        for (size_t i = 0; i < gcells; ++i) grid[i] += tgrid[i];
+      for (int i = 0; i < nband * npol; ++i) sumwt[i] += tsumwt[i];
+      if (js->mode) {
+        for (int i = 0; i < 2 * nband; ++i) sumjones[i] += tsj[i];
+        for (int i = 0; i < 2 * nchan; ++i) sumjones_chan[i] += tsjc[i];
+      }
+    }
+  }
+  if (tid != 0) free(tgrid);
+  free(tsumwt);
+  free(tsj);
+  free(tsjc);
   free(chj);
   free(chq);
+  }
+  free(starts);
   return 0;
 }
 
@@ -386,11 +503,18 @@ int fp64_degrid(const fc *grid, int nband, int npol, int ny, int nx, dc *vis, co
   (void)nrow;
   double n0 = sqrt(1 - l0 * l0 - m0 * m0) - 1;
   size_t nb = (size_t)(uint32_t)bmap[0] + ((size_t)bmap[1] << 32);
-  const int *sizes = bmap + 2, *p = bmap + 2 + nb;
+  const int *sizes = bmap + 2;
+  int64_t *starts = block_starts(bmap, nb);
+  int nthr = 1;
+#ifdef _OPENMP
+  if (nb > 200000) nthr = omp_get_max_threads();
+#endif
+  /* blocks of one map hold disjoint visibilities: parallel over blocks on large maps */
+#pragma omp parallel for num_threads(nthr) schedule(dynamic, 2048)
   for (size_t b = 0; b < nb; ++b) {
+    const int *p = bmap + starts[b];
     int nr = sizes[b] - 2, c0 = p[0], c1 = p[1];
     const int *rows = p + 2;
-    p += sizes[b];
     int gch = chan_map[c0 < nchan ? c0 : 0];
     if (gch < 0 || gch >= nband || nr <= 0 || c1 <= c0) continue;
     double fm = 0, um = 0, vmn = 0, wm = 0;
@@ -406,7 +530,7 @@ int fp64_degrid(const fc *grid, int nband, int npol, int ny, int nx, dc *vis, co
     int64_t cfo;
     int lx, ly, S;
     if (!geometry(nw, overs, ref_wave, wmax, cf_off, cf_sup, nx, ny, incr_x, incr_y, um, vmn, wm, fm / C_LIGHT, &cfo,
-                  &lx, &ly, &S))
+                  &lx, &ly, &S, NULL))
       continue;
     int sup = (S - 1) / 2;
     dc sv[4] = {0, 0, 0, 0};
@@ -448,5 +572,6 @@ int fp64_degrid(const fc *grid, int nband, int npol, int ny, int nx, dc *vis, co
       }
     }
   }
+  free(starts);
   return 0;
 }

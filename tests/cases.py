@@ -164,37 +164,37 @@ def _gpu_objs(c, model_grid=None, vis=None):
     return vs, fg, jd
 
 
-def run_gpu_grid(c, dopsf=False, sorted_=False, compensated=True, chunk=256):
+def run_gpu_grid(c, dopsf=False, batched=False, compensated=False, batch_kw=None):
+    """GPU grid of case c through ddfg_grid, or ddfg_grid_batched (``batched``, with ``batch_kw``
+    for the scheduling); ``compensated`` gives the facet a compensation buffer."""
     import torch
 
     from ddfacet_b200 import device as D
 
     vs, fg, jd = _gpu_objs(c)
-    if sorted_:
-        plan = D.SortPlan.build(vs, [fg], chunk=chunk)
-        D.grid_sorted(vs, [fg], D.make_pol(c.corr_ids, c.stokes_ids), plan, jd, dopsf=dopsf, compensated=compensated)
-    else:
-        D.grid(vs, [fg], D.make_pol(c.corr_ids, c.stokes_ids), jd, dopsf=dopsf)
+    if compensated:
+        fg.with_compensation()
+    batch = D.Batch.create(vs.vis.device, **(batch_kw or {})) if batched else None
+    D.grid(vs, [fg], D.make_pol(c.corr_ids, c.stokes_ids), jd, dopsf=dopsf, batch=batch)
     torch.cuda.synchronize()
     out = {"grid": fg.grid.cpu().numpy(), "sumwt": fg.sumwt.cpu().numpy()}
+    if compensated:
+        out["lo_after"] = float(fg.grid_lo.abs().max().item())
     if c.jones:
         out["sumjones"] = fg.sumjones.cpu().numpy()
         out["sumjones_chan"] = fg.sumjones_chan.cpu().numpy()
     return out
 
 
-def run_gpu_degrid(c, model_grid, vis0=None, sorted_=False, chunk=256):
+def run_gpu_degrid(c, model_grid, vis0=None, batched=False, batch_kw=None):
     import torch
 
     from ddfacet_b200 import device as D
 
     vis = np.zeros_like(c.vis) if vis0 is None else vis0.copy()
     vs, fg, jd = _gpu_objs(c, model_grid=model_grid, vis=vis)
-    if sorted_:
-        plan = D.SortPlan.build(vs, [fg], chunk=chunk)
-        D.degrid_sorted(vs, [fg], D.make_pol(c.corr_ids, c.stokes_ids), plan, jd)
-    else:
-        D.degrid(vs, [fg], D.make_pol(c.corr_ids, c.stokes_ids), jd)
+    batch = D.Batch.create(vs.vis.device, **(batch_kw or {})) if batched else None
+    D.degrid(vs, [fg], D.make_pol(c.corr_ids, c.stokes_ids), jd, batch=batch)
     torch.cuda.synchronize()
     return vs.vis.cpu().numpy()
 

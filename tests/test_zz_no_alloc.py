@@ -6,7 +6,8 @@ start-up): it keeps its scratch in a fixed array inside the library instead of t
 workspace.  This test calls it through the C ABI, twice in a row, and checks that each call's
 block starts equal the workspace-taking entry point's exactly (the plan is integer work), that a
 malformed map is still rejected and a good map after it still plans (the shared error word is
-cleared on every call), and that a map above the fixed limit is refused with a clear error.
+cleared on every call), that a map above the fixed limit is refused with a clear error, and that
+a call leaves the device's free memory unchanged (it allocates nothing).
 Run alone in a fresh process or after the other tests.
 """
 import ctypes as C
@@ -91,3 +92,24 @@ def test_noalloc_refuses_maps_above_its_limit():
     rc, _, _ = _plan_noalloc(lib, m, nrow, nchan, nb=limit + 1)
     assert rc == abi.DDFG_ESIZE
     assert "fixed scratch limit" in abi.last_error()
+
+
+def test_noalloc_call_allocates_no_device_memory():
+    import torch
+
+    lib, abi = _lib()
+    m, nrow, nchan = _maps()[1]
+    nb = int(m[0]) + (int(m[1]) << 32)
+    md = torch.from_numpy(m).cuda()
+    out = torch.full((nb,), -1, dtype=torch.int64, device="cuda")
+    s = torch.cuda.current_stream().cuda_stream
+    single = C.c_int32(-1)
+    assert lib.ddfg_bda_plan_noalloc(md.data_ptr(), md.numel(), nb, nrow, nchan, out.data_ptr(), s,
+                                     C.byref(single)) == 0, abi.last_error()
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info()[0]
+    for _ in range(3):
+        assert lib.ddfg_bda_plan_noalloc(md.data_ptr(), md.numel(), nb, nrow, nchan, out.data_ptr(), s,
+                                         C.byref(single)) == 0, abi.last_error()
+    torch.cuda.synchronize()
+    assert torch.cuda.mem_get_info()[0] == free0
