@@ -1,21 +1,31 @@
 """Benchmark: Mvis/s through one grid+degrid pass over all facets, on synthetic data.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--scale S]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload combined_at_scale|multifacet_dde|uneven_bda] [--scale S] [--no-compensation]
 
-A step is one major-cycle pass of the hot path over the whole visibility set: degrid every
-facet's model grid and subtract the prediction from the visibilities, then grid the residual
-visibilities onto every facet's (zeroed) residual grid.  The workload is the multi-facet DDE
-configuration (81 facets of 735^2, 232 M visibilities x 4 correlations, per-visibility Jones,
-32 w-planes); see ddfacet_b200/configs.py.  Inputs (7.4 GB of visibilities) are larger than L2,
-so no flush is needed between steps.
+Default workload: the combined at-scale configuration -- a 10000^2 image at 1 arcsec in 11 x 11
+facets (121 padded grids of 1485^2), 64 antennas, 8 h at 8 s, 256 channels, 4 correlations,
+1000 point sources + 20 Gaussians, per-facet per-antenna Jones in 5-minute slots, 64 w-planes,
+oversampling 11 (ddfacet_b200/configs.py combined_at_scale) -- streamed in 1-hour chunks.  A step
+is one chunk (232.2 M visibilities x 4 correlations, 7.4 GB) through one major-cycle pass of the
+hot path: degrid every facet's model grid and subtract the prediction from the visibilities, then
+grid the residuals onto every facet's residual grid.  Both calls are the batched ones (one
+persistent, queue-driven launch per call, schedule chosen by ddfacet_b200.autotune) with
+compensated (TwoSum) grid sums unless --no-compensation.  ``plain`` in the JSON line times the same
+kernels one facet per call on the same chunk.  The visibilities (7.4 GB) exceed L2, so no flush is
+needed between steps.
 
-Multi-GPU: the path shards by facet-independent visibility sets, so each rank runs its own
-replica of the workload (weak scaling, no data-path collective); the timed region is bracketed
-by barriers and the maximum over ranks is reported.
+``e2e`` runs the same step through the public API from pinned host buffers: the chunk's
+visibilities, uvw, flags and weights are copied in and the residual visibilities copied out every
+step (pipeline.PipelinedStep, copies overlapped with the kernels).
+
+Multi-GPU: the path shards by chunk (independent visibility sets), so each rank runs its own
+replica (weak scaling, no data-path collective); the timed region is bracketed by barriers and the
+maximum over ranks is reported.
 
 ``--impl reference`` times the reference's own CPU gridder/degridder (oracle/_ref, built from
-DDFacet's sources) on the host cores, one process per facet, on a bounded sample of the same
-workload, and prints the same metric.
+DDFacet's sources) on the host cores, one process per facet, on a bounded row sample of the same
+configuration, and prints the same metric.
 """
 from __future__ import annotations
 
@@ -36,7 +46,8 @@ sys.path.insert(0, ROOT)
 
 METRIC = "Mvis/s grid+degrid on 1 B200, batched vs plain, at <=1e-5 rel err vs FP64"
 UNIT = "Mvis/s"
-E2E_CHUNKS = 8  # time chunks of the end-to-end leg
+E2E_CHUNKS = 4  # sub-chunks of the end-to-end leg (copies of one overlap the kernels of the next)
+C_LIGHT = 299792458.0
 
 
 def _peaks():
@@ -46,6 +57,17 @@ def _peaks():
         return float(p["hbm_gbs"]), "measured"
     except Exception:
         return 6650.0, "fallback"
+
+
+# ------------------------------------------------------------------------------------------
+# Workload descriptions shared by the GPU arm and the CPU reference arm
+# ------------------------------------------------------------------------------------------
+WORKLOADS = {
+    "combined_at_scale": dict(seed=1005, nant=64, radius=4000.0, hours=8.0, dump=8.0, nchan=256, npix=10000,
+                              side=11, cell=1.0, nw=64, chunk_dumps=450, nsrc_cpu=20),
+    "multifacet_dde": dict(seed=1002, nant=64, radius=4000.0, hours=4.0, dump=8.0, nchan=64, npix=4096,
+                           side=9, cell=1.5, nw=32, chunk_dumps=1800, nsrc_cpu=20),
+}
 
 
 # ------------------------------------------------------------------------------------------
@@ -76,44 +98,50 @@ def _cpu_worker(args):
     return dt
 
 
-def cpu_reference(nfacets_total=81, nrow_frac=0.02, nprocs=None, seed=1002):
-    """Reference grid+degrid of the multi-facet DDE workload on a row sample; one process per
-    facet on the host cores.  Returns (Mvis/s for the full job, cores, sample description)."""
+def cpu_reference(workload="combined_at_scale", nrow_frac=0.005, nprocs=None):
+    """The reference's grid+degrid of the workload's chunk on a row sample, one process per facet
+    on the host cores, extrapolated to every row and facet of the chunk.  Returns (Mvis/s, cores,
+    sample description)."""
     from ddfacet_b200 import bda, cf, geometry, synth
 
+    p = WORKLOADS[workload]
+    nchan = p["nchan"]
     ncpu = os.cpu_count() or 1
+    tess = geometry.regular_facets(p["npix"], p["side"], p["cell"], 1.7)
+    nfacets_total = len(tess.facets)
     nprocs = nprocs or min(ncpu, nfacets_total)
-    nchan = 64
-    obs = synth.make_observation(seed, 64, 4000.0, 34.0, 40.0, 4.0, 8.0, nchan, 0.90e9, 1.67e9)
-    tess = geometry.regular_facets(4096, 9, 1.5, 1.7)
-    nrow_s = max(1, int(obs.nrow * nrow_frac))
+    full = synth.make_observation(p["seed"], p["nant"], p["radius"], 34.0, 40.0, p["hours"], p["dump"], nchan,
+                                  0.90e9, 1.67e9)
+    wmax = float(np.max(np.abs(full.uvw[:, 2]))) * 1.001
+    chunk_rows = p["chunk_dumps"] * full.nbl
+    nrow_s = max(full.nbl, int(chunk_rows * nrow_frac))
     rows = np.arange(nrow_s)
-    uvw = obs.uvw[rows].copy()
-    l, m, s = synth.point_sky(seed + 1, 20, tess.npix * tess.cell_rad / 2 * 0.95, flux=("powerlaw", 1e-3, 1.0))
-    rng = np.random.default_rng(seed + 2)
-    vis = synth.add_noise(rng, synth.dft_predict(uvw, obs.freqs, l, m, s, ncorr=4), 1e-3).astype(np.complex64)
+    uvw = full.uvw[rows].copy()
+    l, m, s = synth.point_sky(p["seed"] + 1, p["nsrc_cpu"], tess.npix * tess.cell_rad / 2 * 0.95,
+                              flux=("powerlaw", 1e-3, 1.0))
+    rng = np.random.default_rng(p["seed"] + 2)
+    vis = synth.add_noise(rng, synth.dft_predict(uvw, full.freqs, l, m, s, ncorr=4), 1e-3).astype(np.complex64)
     flags = np.zeros(vis.shape, bool)
     weights = np.ones((nrow_s, nchan), np.float32)
-    bmap = bda.plain_map(obs.A0[rows], obs.A1[rows], nchan)
-    nt = int(np.ceil(4.0 * 3600 / 300.0))
-    J = synth.random_jones(seed + 3, nt, len(tess.facets), 64, 1, 0.1)
-    tmap = np.minimum(((obs.times[rows] - obs.times.min()) // 300.0).astype(np.int32), nt - 1)
-    wmax = float(np.max(np.abs(obs.uvw[:, 2]))) * 1.001
-    cell = 1.5
+    bmap = bda.plain_map(full.A0[rows], full.A1[rows], nchan)
+    nt = int(np.ceil(p["hours"] * 3600 / 300.0))
+    J = synth.random_jones(p["seed"] + 3, nt, nfacets_total, p["nant"], 1, 0.1)
+    tmap = np.minimum(((full.times[rows] - full.times.min()) // 300.0).astype(np.int32), nt - 1)
+    cell = p["cell"]
     facets = []
-    pick = [tess.facets[i] for i in np.linspace(0, len(tess.facets) - 1, nprocs).astype(int)]
+    pick = [tess.facets[i] for i in np.linspace(0, nfacets_total - 1, nprocs).astype(int)]
     for fgeo in pick:
-        wt = cf.WTerms(Cell=cell, Sup=7, Nw=32, wmax=wmax, Npix=tess.npix_padded, Freqs=obs.freqs, OverS=11,
+        wt = cf.WTerms(Cell=cell, Sup=7, Nw=p["nw"], wmax=wmax, Npix=tess.npix_padded, Freqs=full.freqs, OverS=11,
                        lmShift=(fgeo.l0, fgeo.m0))
         model = (rng.standard_normal((1, 1, tess.npix_padded, tess.npix_padded)) * 1e-3).astype(np.complex64)
-        facets.append(dict(wp=wt.Wplanes, wc=wt.WplanesConj, winfos=np.array([wt.RefWave, wt.wmax, 32, 11.]),
+        facets.append(dict(wp=wt.Wplanes, wc=wt.WplanesConj, winfos=np.array([wt.RefWave, wt.wmax, p["nw"], 11.]),
                            finfo=np.array([wt.Cu, wt.Cv, fgeo.l0, fgeo.m0, fgeo.index]), idir=fgeo.index,
                            model=model))
-    d = dict(vis=vis, uvw=uvw, flags=flags, weights=weights, freqs=obs.freqs, chan_map=np.zeros(nchan, np.int32),
+    d = dict(vis=vis, uvw=uvw, flags=flags, weights=weights, freqs=full.freqs, chan_map=np.zeros(nchan, np.int32),
              bda=bmap, corr=[9, 10, 11, 12], stokes=[1], npix=tess.npix_padded, nrow=nrow_s, nchan=nchan,
              incr=np.array([-cell, cell]) / 3600 * np.pi / 180, facets=facets,
-             jones=dict(kms=J, kms_tmap=tmap, kms_cmap=np.zeros(nchan, np.int32), A0=obs.A0[rows].astype(np.int32),
-                        A1=obs.A1[rows].astype(np.int32), mode=1, interp_mode=0, apply_amp=1, apply_phase=1,
+             jones=dict(kms=J, kms_tmap=tmap, kms_cmap=np.zeros(nchan, np.int32), A0=full.A0[rows].astype(np.int32),
+                        A1=full.A1[rows].astype(np.int32), mode=1, interp_mode=0, apply_amp=1, apply_phase=1,
                         scale=0, calib_err=0.0))
     fd, path = tempfile.mkstemp(suffix=".npy", dir="/dev/shm" if os.path.isdir("/dev/shm") else None)
     os.close(fd)
@@ -128,15 +156,92 @@ def cpu_reference(nfacets_total=81, nrow_frac=0.02, nprocs=None, seed=1002):
         os.unlink(path)
     nvis_s = nrow_s * nchan
     # nprocs facets processed concurrently, each timed around its grid+degrid calls (the slowest
-    # bounds the round); the full job is nfacets_total facets over all rows.
+    # bounds the round); the job is every facet over every row of the chunk.
     per_facet_vis_rate = nprocs * nvis_s / max(max(times), 1e-9)  # facet-visibilities per second
-    full_nvis = obs.nrow * nchan
-    job_time = full_nvis * nfacets_total / per_facet_vis_rate
-    mvis = full_nvis / job_time / 1e6
-    sample = (f"{nrow_s} rows x {nchan} ch x 4 corr ({nvis_s/1e6:.2f} Mvis) of the {obs.nrow}-row set, "
-              f"{nprocs} of {nfacets_total} facets in parallel (one process each), grid+degrid with per-vis Jones, "
-              f"wall {wall:.2f}s (per-process {min(times):.2f}-{max(times):.2f}s), scaled to all rows and facets")
+    chunk_nvis = chunk_rows * nchan
+    job_time = chunk_nvis * nfacets_total / per_facet_vis_rate
+    mvis = chunk_nvis / job_time / 1e6
+    sample = (f"{nrow_s} rows x {nchan} ch x 4 corr ({nvis_s/1e6:.2f} Mvis, {p['nsrc_cpu']}-source sky + noise) "
+              f"of the {chunk_rows}-row chunk, {nprocs} of {nfacets_total} facets in parallel (one process each), "
+              f"grid+degrid with per-vis Jones, wall {wall:.2f}s (per-process {min(times):.2f}-{max(times):.2f}s), "
+              "scaled to all rows and facets of the chunk")
     return mvis, nprocs, sample
+
+
+def err_vs_fp64(w, compensated, pick=(0, None), sample_rows=None):
+    """Errors of the GPU path against the FP64 restatement (oracle/gridder_fp64.c) on the benchmark's
+    own data: the grid of a corner and the centre facet over every row of the chunk (the full
+    accumulation depth), and the prediction of the same facets on a row sample."""
+    import torch
+
+    from ddfacet_b200 import device as D
+    from oracle import fp64
+
+    nf = w.nfacets
+    pick = [0, nf // 2] if pick == (0, None) else list(pick)
+    obs = w.host["obs"]
+    dev = w.vs.vis.device
+    vis_h = w.vs.vis.cpu().numpy()
+    bmap_h = w.vs.bda_map.cpu().numpy()
+    flags = np.zeros(vis_h.shape, bool)
+    weights = np.ones(vis_h.shape[:2], np.float32)
+    jh = {"A0": obs.A0.astype(np.int32), "A1": obs.A1.astype(np.int32), "mode": 1, "interp_mode": 0, "apply_amp": 1,
+          "apply_phase": 1, "scale": 0, "calib_err": 0.0, "idir_beam": 0, "kms": w.host["J"],
+          "kms_tmap": w.host["tmap"], "kms_cmap": np.zeros(w.nchan, np.int32)}
+    out = {"grid": {}, "degrid": {}}
+    t0 = time.perf_counter()
+    fs = [w.facets_grid[i] for i in pick]
+    saved = [(f.grid.clone(), f.grid_lo) for f in fs]
+    for f in fs:
+        f.grid.zero_()
+        f.grid_lo = None
+        if compensated:
+            f.with_compensation()
+    D.grid(w.vs, fs, w.pol, w.jones, batch=D.Batch.create(dev))
+    torch.cuda.synchronize()
+    gpu_grids = [f.grid.cpu().numpy() for f in fs]
+    for f, (g, lo) in zip(fs, saved):
+        f.grid.copy_(g)
+        f.grid_lo = lo
+    for i, g in zip(pick, gpu_grids):
+        wt = w.host["wterms"][i]
+        fgeo = w.host["tess"].facets[i]
+        ref64 = fp64.grid(vis_h, obs.uvw, flags, weights, obs.freqs, w.host["chan_map"], bmap_h, wt.Wplanes,
+                          wt.WplanesConj, 11, wt.RefWave, wt.wmax, w.facets_grid[i].incr, wt.Cu, wt.Cv,
+                          (fgeo.l0, fgeo.m0), [9, 10, 11, 12], [1], 1, w.info["npix_padded"],
+                          jones=dict(jh, idir_kms=w.facets_grid[i].idir_kms))[0]
+        d = g.astype(np.complex128) - ref64
+        out["grid"][str(i)] = float(np.sqrt(np.mean(np.abs(d) ** 2) / np.mean(np.abs(ref64) ** 2)))
+    # prediction on a row sample: degrid the picked facets into zeros
+    from ddfacet_b200 import bda
+
+    nr = sample_rows or max(obs.nbl, min(obs.nrow, 64 * obs.nbl))
+    zeros = torch.zeros((nr, w.nchan, w.ncorr), dtype=torch.complex64, device=dev)
+    bm = bda.plain_map(obs.A0[:nr], obs.A1[:nr], w.nchan)
+    vs_s = D.VisData.create(zeros, w.vs.uvw[:nr], w.vs.flags[:nr], w.vs.weights[:nr], obs.freqs, w.host["chan_map"],
+                            bm, device=dev)
+    jd = dict(jh, A0=jh["A0"][:nr], A1=jh["A1"][:nr], kms_tmap=jh["kms_tmap"][:nr])
+    from ddfacet_b200 import pipeline
+
+    D.degrid(vs_s, [w.facets_model[i] for i in pick], w.pol, pipeline.jones_rows(w.jones, 0, nr),
+             batch=D.Batch.create(dev))
+    torch.cuda.synchronize()
+    got = vs_s.vis.cpu().numpy().astype(np.complex128)
+    want = np.zeros_like(got)
+    for i in pick:
+        wt = w.host["wterms"][i]
+        fgeo = w.host["tess"].facets[i]
+        want += fp64.degrid(w.facets_model[i].grid.cpu().numpy(), np.zeros_like(got), obs.uvw[:nr], obs.freqs,
+                            w.host["chan_map"], bm, wt.Wplanes, wt.WplanesConj, 11, wt.RefWave, wt.wmax,
+                            w.facets_model[i].incr, wt.Cu, wt.Cv, (fgeo.l0, fgeo.m0), [9, 10, 11, 12], [1],
+                            jones=dict(jd, idir_kms=w.facets_model[i].idir_kms))
+    out["degrid"]["facets " + ",".join(map(str, pick))] = float(
+        np.sqrt(np.mean(np.abs(got - want) ** 2) / np.mean(np.abs(want) ** 2)))
+    out["max"] = max(list(out["grid"].values()) + list(out["degrid"].values()))
+    out["how"] = (f"grid: facets {pick} over all {obs.nrow} rows of the chunk ({w.nvis/1e6:.1f} Mvis) against the "
+                  f"FP64 restatement; degrid: the same facets' summed prediction on the first {nr} rows; "
+                  f"relative RMS; {time.perf_counter() - t0:.0f} s on {os.cpu_count()} host threads")
+    return out
 
 
 # ------------------------------------------------------------------------------------------
@@ -190,18 +295,60 @@ def tap_stats(w, sample_rows=20000):
     rows = np.linspace(0, obs.nrow - 1, min(sample_rows, obs.nrow)).astype(int)
     wabs = np.abs(obs.uvw[rows, 2])[:, None]
     nu = obs.freqs[None, :]
-    iw = np.rint((wt.Nw - 1) * wabs * (wt.RefWave * nu / 299792458.0) / wt.wmax).astype(int)
+    iw = np.rint((wt.Nw - 1) * wabs * (wt.RefWave * nu / C_LIGHT) / wt.wmax).astype(int)
     sups = np.array([p.shape[0] // 11 for p in wt.Wplanes])
     ok = iw < len(sups)
     s2 = np.where(ok, sups[np.minimum(iw, len(sups) - 1)] ** 2, 0)
     return float(s2.mean())
 
 
+def fp32_peak_tflops(dev):
+    """FP32 (CUDA-core) dense throughput measured with a cuBLAS SGEMM (TF32 off), TFLOP/s."""
+    import torch
+
+    old = torch.backends.cuda.matmul.allow_tf32
+    torch.backends.cuda.matmul.allow_tf32 = False
+    try:
+        n = 8192
+        a = torch.randn((n, n), device=dev)
+        b = torch.randn((n, n), device=dev)
+        torch.mm(a, b)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        best = float("inf")
+        for _ in range(5):
+            e0.record()
+            torch.mm(a, b)
+            e1.record()
+            torch.cuda.synchronize()
+            best = min(best, e0.elapsed_time(e1))
+        del a, b
+        return 2 * n ** 3 / (best * 1e-3) / 1e12
+    finally:
+        torch.backends.cuda.matmul.allow_tf32 = old
+
+
+def algorithmic(w, s2):
+    """Compulsory bytes and FLOPs of one grid call and one degrid call (one pass over the chunk):
+    every stream touched once.  Grid: visibilities (K complex64), flags (K bytes), weights, uvw,
+    the residual grids written, one CF table set, the Jones array.  Degrid: visibilities read and
+    written, uvw, the model grids read, CF, Jones.  FLOPs: S^2 complex multiply-adds per facet and
+    visibility (8 flops each) plus the 2x2 Jones products (112) and phasor/weight (20)."""
+    K, F = w.ncorr, w.nfacets
+    G2 = sum(int(f.grid.numel()) for f in w.facets_grid)
+    cf_bytes = sum(int(f.cf.data.numel()) * 8 for f in w.facets_grid) // 2
+    jones_bytes = int(w.jones.kms.numel()) * 8 if w.jones is not None else 0
+    grid_b = w.nvis * (K * 8 + K + 4) + w.nrow * 24 + G2 * 8 + cf_bytes + jones_bytes
+    degrid_b = w.nvis * (K * 16) + w.nrow * 24 + G2 * 8 + cf_bytes + jones_bytes
+    flops_call = F * w.nvis * (8 * s2 + 112 + 20)
+    return grid_b, degrid_b, flops_call
+
+
 def run_gpu(args):
     import torch
     import torch.distributed as dist
 
-    from ddfacet_b200 import configs, device as D, pipeline
+    from ddfacet_b200 import autotune, configs, device as D, pipeline
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -213,29 +360,40 @@ def run_gpu(args):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     dev = torch.device("cuda", local if world > 1 else 0)
     torch.cuda.set_device(dev)
+    comp = not args.no_compensation
 
     t_build = time.perf_counter()
-    w = configs.multifacet_dde(device=dev, scale=args.scale)
+    if args.workload == "multifacet_dde":
+        w = configs.multifacet_dde(device=dev, scale=args.scale)
+    else:
+        w = configs.combined_at_scale(device=dev, scale=args.scale)
+    if comp:
+        for f in w.facets_grid:
+            f.with_compensation()
     torch.cuda.synchronize()
     t_build = time.perf_counter() - t_build
     stream = torch.cuda.current_stream()
-    fpl = 16
+
+    t_tune = time.perf_counter()
+    tuned = autotune.tune(w.vs, w.facets_grid, w.facets_model, w.pol, w.jones, use_cache=not args.retune)
+    t_tune = time.perf_counter() - t_tune
+    bg, bd = tuned.grid, tuned.degrid
 
     def step(ev=None):
         for f in w.facets_grid:
             f.grid.zero_()
         if ev:
             ev[0].record(stream)
-        D.degrid(w.vs, w.facets_model, w.pol, w.jones)
+        D.degrid(w.vs, w.facets_model, w.pol, w.jones, batch=bd)
         if ev:
             ev[1].record(stream)
-        D.grid(w.vs, w.facets_grid, w.pol, w.jones)
+        D.grid(w.vs, w.facets_grid, w.pol, w.jones, batch=bg)
         if ev:
             ev[2].record(stream)
 
     def plain_step():
-        # the same physics with one facet per launch, blocks in map order (direct kernels)
-        for fm, fg in zip(w.facets_model, w.facets_grid):
+        # the same kernels with one facet per call (one launch per facet and direction)
+        for fm in w.facets_model:
             D.degrid(w.vs, [fm], w.pol, w.jones)
         for fg in w.facets_grid:
             fg.grid.zero_()
@@ -269,6 +427,8 @@ def run_gpu(args):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms_total = float(t.item())
     ms_step = ms_total / args.steps
+    degrid_ms = float(np.mean([e[0].elapsed_time(e[1]) for e in evs]))
+    grid_ms = float(np.mean([e[1].elapsed_time(e[2]) for e in evs]))
 
     # The same step captured once in a CUDA graph and replayed (device.capture_graph).
     graph = D.capture_graph(step)
@@ -276,24 +436,22 @@ def run_gpu(args):
     gr0 = torch.cuda.Event(enable_timing=True)
     gr1 = torch.cuda.Event(enable_timing=True)
     gr0.record(stream)
-    for _ in range(max(1, min(args.steps, 3))):
-        graph.replay()
+    graph.replay()
     gr1.record(stream)
     torch.cuda.synchronize()
-    graph_ms = gr0.elapsed_time(gr1) / max(1, min(args.steps, 3))
+    graph_ms = gr0.elapsed_time(gr1)
     del graph
-    degrid_ms = float(np.mean([e[0].elapsed_time(e[1]) for e in evs]))
-    grid_ms = float(np.mean([e[1].elapsed_time(e[2]) for e in evs]))
 
     # End to end through the public API with host buffers: every step copies its inputs from
-    # pinned memory and its residual visibilities back, in E2E_CHUNKS time chunks whose copies
-    # overlap the kernels of the neighbouring chunk (pipeline.PipelinedStep).
+    # pinned memory and its residual visibilities back, in E2E_CHUNKS sub-chunks whose copies
+    # overlap the kernels of the neighbouring sub-chunk (pipeline.PipelinedStep).
     host = {"vis": w.host["vis"], "uvw": w.vs.uvw.cpu().pin_memory(), "flags": w.vs.flags.cpu().pin_memory(),
             "weights": w.vs.weights.cpu().pin_memory()}
     host["out"] = torch.empty_like(host["vis"]).pin_memory()
     h2d = (host["vis"].numel() * 8 + host["uvw"].numel() * 8 + host["flags"].numel() + host["weights"].numel() * 4)
     d2h = host["out"].numel() * 8
-    piped = pipeline.PipelinedStep(configs.row_chunks(w, E2E_CHUNKS), w.facets_grid, w.facets_model, w.pol, dev)
+    piped = pipeline.PipelinedStep(configs.row_chunks(w, E2E_CHUNKS), w.facets_grid, w.facets_model, w.pol, dev,
+                                   batch_grid=bg, batch_degrid=bd)
 
     def e2e_step():
         for f in w.facets_grid:
@@ -317,122 +475,72 @@ def run_gpu(args):
         t = torch.tensor([e2e_ms], device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_ms = float(t.item())
+    del piped
 
-    # Imaging weights (Briggs, robust 0) of the same visibilities: index, density accumulation,
-    # Briggs transform and normalisation, device-resident, timed on the device.
-    from ddfacet_b200.weights import ImagingWeights, uvmax_wavelengths
-    obs = w.host["obs"]
-    uvmax = uvmax_wavelengths(w.vs.uvw, None, obs.freqs)
-    tess = w.host["tess"]
-
-    def weights_pass():
-        iw = ImagingWeights(uvmax, tess.cell_rad, tess.npix, mode="briggs", robust=0.0, device=dev)
-        iw.accumulate(w.vs.uvw, obs.freqs, w.vs.weights)
-        iw.finish()
-        return iw, iw.apply(w.vs.uvw, obs.freqs, w.vs.weights)
-
-    weights_pass()
+    # The plain path on the same chunk: one facet per call.
+    plain_step()
     torch.cuda.synchronize()
-    q0 = torch.cuda.Event(enable_timing=True)
-    q1 = torch.cuda.Event(enable_timing=True)
-    q0.record(stream)
-    iw, _ = weights_pass()
-    q1.record(stream)
+    p0 = torch.cuda.Event(enable_timing=True)
+    p1 = torch.cuda.Event(enable_timing=True)
+    p0.record(stream)
+    plain_step()
+    p1.record(stream)
     torch.cuda.synchronize()
-    weights_ms = q0.elapsed_time(q1)
-    # bytes: uvw and weights read twice (index for accumulation, index for normalisation), index
-    # written and read twice, weights written once; the density grid is small and L2-resident
-    wbytes = 2 * (w.nrow * 24 + nvis_w(w) * 4) + 4 * nvis_w(w) * 4 + nvis_w(w) * 4
-    weights_info = {"ms": round(weights_ms, 3), "Mvis_per_s": round(w.nvis / (weights_ms * 1e-3) / 1e6, 1),
-                    "achieved_GBs": round(wbytes / (weights_ms * 1e-3) / 1e9, 1),
-                    "grid": [int(iw.npixx), int(iw.npixy)], "mode": "briggs robust 0"}
-    del iw
-
-    # Mode-1 BDA block map (DDFacet's default averaging, GridDecorr 0.02) of the same rows, built
-    # on the GPU; reported beside the metric (the timed step itself uses single-visibility blocks).
-    from ddfacet_b200 import bda as bda_mod
-    dfreq = float(obs.freqs[1] - obs.freqs[0])
-    lmax = tess.npix * tess.cell_rad * np.sqrt(2) / 2
-    bargs = (obs.A0, obs.A1, w.vs.uvw, obs.freqs, dfreq, np.sqrt(6 * 0.02), lmax, w.host["chan_map"])
-    bda_mod.smear_mapping_gpu(*bargs)
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    bmap = bda_mod.smear_mapping_gpu(*bargs)
-    torch.cuda.synchronize()
-    bda_ms = (time.perf_counter() - t0) * 1e3
-    nb_bda = int(bmap[0].item()) & 0xFFFFFFFF
-    bda_info = {"ms": round(bda_ms, 2), "blocks": nb_bda, "vis_per_block": round(w.nvis / max(nb_bda, 1), 2),
-                "what": "mode-1 map, GridDecorr 0.02, l = image radius x sqrt 2, wall time incl. host grouping"}
-    del bmap
+    plain_ms = p0.elapsed_time(p1)
 
     # Differentiation (the prediction as a torch.autograd.Function, ddfacet_b200.autograd): the
     # forward prediction, then the backward passes for every facet's model grid (adjoint gridding
     # kernel) and the per-facet per-antenna Jones, timed on the device.
     diff_info = None
-    if w.jones is not None:
+    if w.jones is not None and not args.no_diff:
         from ddfacet_b200.autograd import PredictSetup, predict
         setup = PredictSetup(vs=w.vs, facets=w.facets_model, pol=w.pol, jones=w.jones)
         leaves = [f.grid.detach().clone().requires_grad_(True) for f in w.facets_model]
         kms_leaf = w.jones.kms.detach().clone().requires_grad_(True)
-
-        def diff_pass(ev=None):
-            if ev:
-                ev[0].record(stream)
-            P = predict(setup, leaves, kms_leaf)
-            if ev:
-                ev[1].record(stream)
-            grads = torch.autograd.grad(P, [*leaves, kms_leaf], grad_outputs=w.vs.vis)
-            if ev:
-                ev[2].record(stream)
-            return grads
-
-        diff_pass()
-        torch.cuda.synchronize()
         de = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
-        grads = diff_pass(de)
+        de[0].record(stream)
+        P = predict(setup, leaves, kms_leaf)
+        de[1].record(stream)
+        grads = torch.autograd.grad(P, [*leaves, kms_leaf], grad_outputs=w.vs.vis)
+        de[2].record(stream)
         torch.cuda.synchronize()
         fwd_ms, bwd_ms = de[0].elapsed_time(de[1]), de[1].elapsed_time(de[2])
-        del grads, leaves, kms_leaf
+        del grads, leaves, kms_leaf, P
         diff_info = {"forward_ms": round(fwd_ms, 1), "backward_ms": round(bwd_ms, 1),
                      "Mvis_per_s": round(w.nvis / ((fwd_ms + bwd_ms) * 1e-3) / 1e6, 2),
                      "what": "predict (all facets) + backward for all model grids and the kMS Jones"}
-
-    plain_ms = None
-    if args.plain:
-        plain_step()
-        torch.cuda.synchronize()
-        p0 = torch.cuda.Event(enable_timing=True)
-        p1 = torch.cuda.Event(enable_timing=True)
-        p0.record(stream)
-        plain_step()
-        p1.record(stream)
-        torch.cuda.synchronize()
-        plain_ms = p0.elapsed_time(p1)
+        torch.cuda.empty_cache()
 
     nvis = w.nvis
     value = world * nvis / (ms_step * 1e-3) / 1e6
     e2e_value = world * nvis / (e2e_ms * 1e-3) / 1e6
+    plain_value = world * nvis / (plain_ms * 1e-3) / 1e6
 
-    # Roofline of the dominant kernel: algorithmic bytes per call (inputs read once per 16-facet
-    # launch, grids and CF tables once per call).
-    K = w.ncorr
-    F = w.nfacets
-    G = w.info["npix_padded"]
-    cf_bytes = sum(int(f.cf.data.numel()) * 8 for f in w.facets_grid)
-    jones_bytes = int(w.jones.kms.numel()) * 8 if w.jones is not None else 0
-    launches_per_call = math.ceil(F / (fpl if fpl > 0 else 16))
-    grid_bytes = (launches_per_call * (nvis * (K * 8 + K + 4) + w.nrow * 24 + jones_bytes)
-                  + F * G * G * 8 * 2 + cf_bytes // 2)
-    degrid_bytes = (launches_per_call * (nvis * (K * 16) + w.nrow * 24 + jones_bytes)
-                    + F * G * G * 8 + cf_bytes // 2)
     s2 = tap_stats(w)
-    flops_pass = F * nvis * (2 * s2 * 8 + 2 * (112 + 40))
+    grid_b, degrid_b, flops_call = algorithmic(w, s2)
     hbm_peak, peak_kind = _peaks()
+    fp32_peak = fp32_peak_tflops(dev)
     dom = "grid" if grid_ms >= degrid_ms else "degrid"
     dom_ms = max(grid_ms, degrid_ms)
-    dom_bytes = grid_bytes if dom == "grid" else degrid_bytes
+    dom_bytes = grid_b if dom == "grid" else degrid_b
     achieved = dom_bytes / (dom_ms * 1e-3) / 1e9
-    fp32_peak = 148 * 128 * 2 * 1.965e9 / 1e12
+    # DRAM bytes (read + write) per launch of the dominant kernel, from the ncu capture of the
+    # 0.02-scale chunk (profiles/), per visibility, scaled to this chunk's visibilities
+    traffic_per_vis = {"grid": 192.0, "degrid": 60.0}
+    K, F, G = w.ncorr, w.nfacets, w.info["npix_padded"]
+    launches_grid = math.ceil(F / 128) * (2 if comp else 1)
+    dpp = bd.facets_per_pack if bd.facets_per_pack > 0 else 128
+    launches_degrid = math.ceil(F / min(dpp, 128))
+    desc = {
+        "combined_at_scale": (f"combined at scale, one 1-h chunk: {F} facets x {G}^2 grids, {w.nrow} rows x "
+                              f"{w.nchan} ch x {K} corr ({nvis/1e6:.1f} Mvis, 7.4 GB) of the 8-h track "
+                              f"({w.info['full_track_nvis']/1e9:.2f} G vis in 8 chunks), per-vis Jones, "
+                              f"{w.info['nw']} w-planes, OverS 11, 1000 point + 20 Gaussian sources; step = degrid "
+                              "all facets (subtract) + grid all facets"),
+        "multifacet_dde": (f"multi-facet DDE: {F} facets x {G}^2 grid, {w.nrow} rows x {w.nchan} ch x {K} corr "
+                           f"({nvis/1e6:.1f} Mvis), per-vis Jones, {w.info['nw']} w-planes, OverS 11; step = degrid "
+                           "all facets (subtract) + grid all facets"),
+    }[args.workload]
     out = {
         "metric": METRIC,
         "value": round(value, 3),
@@ -444,44 +552,43 @@ def run_gpu(args):
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
-        "dtype": "f32 (FP64 phase/index arithmetic)",
+        "dtype": "f32" + (" (compensated grid sums)" if comp else "") + "; FP64 phase/index arithmetic",
         "data": "synthetic (seeded; generated on device)",
         "config": {
-            "workload": f"multi-facet DDE: {F} facets x {G}^2 grid, {w.nrow} rows x {w.nchan} ch x {K} corr "
-                        f"({nvis/1e6:.1f} Mvis), per-vis Jones, {w.info['nw']} w-planes, OverS 11; "
-                        "step = degrid all facets (subtract) + grid all facets",
-            "facets": F, "grid": G, "nvis": nvis, "ncorr": K, "nchan": w.nchan, "nrow": w.nrow,
-            "w_planes": w.info["nw"], "mean_taps_per_vis": round(s2, 1),
-            "l2": "inputs (7.4 GB visibilities) larger than L2; no flush",
+            "workload": desc, "facets": F, "grid": G, "nvis": nvis, "ncorr": K, "nchan": w.nchan, "nrow": w.nrow,
+            "w_planes": w.info["nw"], "supports": w.info["supports"], "mean_taps_per_vis": round(s2, 1),
+            "array": "64 antennas uniform in a disk of 4 km radius (the '8 km disk' read as its diameter)",
+            "bda": "none: every (row, channel) its own block",
+            "chunk": w.info.get("chunk", "whole set"),
+            "l2": f"inputs ({nvis * K * 8 / 1e9:.1f} GB visibilities) larger than L2; no flush",
             "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
             "scale": args.scale,
+            "compensated": comp,
         },
         "kernels_ms": {"degrid_call": round(degrid_ms, 3), "grid_call": round(grid_ms, 3),
                        "graph_replay_step": round(graph_ms, 3)},
-        "plain": (None if plain_ms is None else
-                  {"ms_per_step": round(plain_ms, 1), "value": round(world * nvis / (plain_ms * 1e-3) / 1e6, 3),
-                   "what": "the same kernels, one facet per call (one launch per facet and direction)",
-                   "batched_speedup": round(plain_ms / ms_step, 2)}),
-        "facets_per_launch": fpl,
-        "bda_map": bda_info,
+        "plain": {"ms_per_step": round(plain_ms, 1), "value": round(plain_value, 3),
+                  "what": "the same kernels, one facet per call (one launch per facet and direction), same chunk",
+                  "batched_speedup": round(plain_ms / ms_step, 3)},
+        "schedule": dict(tuned.describe(), tune_s=round(t_tune, 1)),
         "differentiation": diff_info,
-        "imaging_weights": dict(weights_info, frac_of_hbm=round(weights_info["achieved_GBs"] / _peaks()[0], 4)),
         "roofline": {
             "bound": "hbm", "kernel": dom, "achieved": round(achieved, 2), "peak": hbm_peak, "unit": "GB/s",
-            "frac": round(achieved / hbm_peak, 5), "peak_kind": peak_kind,
-            # DRAM bytes (read + write) of one 16-facet launch of the dominant kernel: 95.0 B per
-            # visibility (grid) / 113 B (degrid), measured by ncu on the 0.05-scale workload and
-            # scaled by visibilities
-            "traffic": int((95.0 if dom == "grid" else 113.0) * nvis),
-            "alg_bytes_per_launch": int(dom_bytes / launches_per_call),
-            "fp32": {"achieved_tflops": round(flops_pass / (ms_step * 1e-3) / 1e12, 2),
-                     "peak_tflops_nominal": round(fp32_peak, 1),
-                     "frac": round(flops_pass / (ms_step * 1e-3) / 1e12 / fp32_peak, 4)},
+            "frac": round(achieved / hbm_peak, 6), "peak_kind": peak_kind,
+            "traffic": int(traffic_per_vis[dom] * nvis),
+            "alg_bytes_per_launch": int(dom_bytes),
+            "how": ("achieved = compulsory bytes of one call (visibilities, flags, weights, uvw, grids, one CF "
+                    "table set, Jones; one launch per call) / the call's CUDA-event time; traffic = DRAM "
+                    "read+write per visibility of the ncu capture (0.02-scale chunk) x visibilities"),
+            "fp32": {"achieved_tflops": round(flops_call / (dom_ms * 1e-3) / 1e12, 3),
+                     "peak_tflops": round(fp32_peak, 1), "peak_kind": "measured (cuBLAS SGEMM, TF32 off)",
+                     "frac": round(flops_call / (dom_ms * 1e-3) / 1e12 / fp32_peak, 4),
+                     "flops_per_call": int(flops_call)},
         },
         "e2e": {"value": round(e2e_value, 3), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h), "ms_per_step": round(e2e_ms, 3),
-                "how": f"pinned host buffers, {E2E_CHUNKS} time chunks, copies overlapped with the kernels"},
-        "gpu_launches": args.steps * 2 * launches_per_call,
+                "how": f"pinned host buffers, {E2E_CHUNKS} sub-chunks, copies overlapped with the kernels"},
+        "gpu_launches": args.steps * (launches_grid + launches_degrid),
         "clocks": clk.summary(),
         "setup_s": round(t_build, 1),
     }
@@ -489,23 +596,25 @@ def run_gpu(args):
         dist.barrier()
         dist.destroy_process_group()
     if rank == 0 and args.cpu_baseline and world == 1:
-        mv, cores, sample = cpu_reference(F)
-        out["cpu_baseline"] = {"value": round(mv, 4), "unit": UNIT, "cores": cores, "kind": "reference",
-                               "sample": sample}
+        torch.cuda.empty_cache()
+        try:
+            out["err_vs_fp64"] = err_vs_fp64(w, comp)
+        except Exception as e:  # the check is reported, not allowed to drop the measurement
+            out["err_vs_fp64"] = {"error": repr(e)[:300]}
+        if args.workload in WORKLOADS:
+            mv, cores, sample = cpu_reference(args.workload)
+            out["cpu_baseline"] = {"value": round(mv, 4), "unit": UNIT, "cores": cores, "kind": "reference",
+                                   "sample": sample}
     if rank == 0:
         print(json.dumps(out), flush=True)
 
 
-def nvis_w(w):
-    return w.nrow * w.nchan
-
-
 def run_uneven(args):
-    """Uneven Voronoi facets with averaged BDA blocks (an additional workload, not the metric's
-    configuration): one degrid + grid step over all facets, device-resident, CUDA-event timed."""
+    """Uneven Voronoi facets with averaged BDA blocks (the batching-form workload): one degrid + grid
+    step over all facets, device-resident, CUDA-event timed, batched and plain."""
     import torch
 
-    from ddfacet_b200 import configs, device as D
+    from ddfacet_b200 import autotune, configs, device as D
 
     dev = torch.device("cuda", 0)
     t0 = time.perf_counter()
@@ -513,28 +622,45 @@ def run_uneven(args):
     torch.cuda.synchronize()
     setup_s = time.perf_counter() - t0
     stream = torch.cuda.current_stream()
+    tuned = autotune.tune(w.vs, w.facets_grid, w.facets_model, w.pol, w.jones, use_cache=not args.retune)
 
-    def step():
+    def step(batched=True):
         for f in w.facets_grid:
             f.grid.zero_()
-        D.degrid(w.vs, w.facets_model, w.pol, w.jones)
-        D.grid(w.vs, w.facets_grid, w.pol, w.jones)
+        if batched:
+            D.degrid(w.vs, w.facets_model, w.pol, w.jones, batch=tuned.degrid)
+            D.grid(w.vs, w.facets_grid, w.pol, w.jones, batch=tuned.grid)
+        else:
+            for fm in w.facets_model:
+                D.degrid(w.vs, [fm], w.pol, w.jones)
+            for fg in w.facets_grid:
+                D.grid(w.vs, [fg], w.pol, w.jones)
+
+    def timed(batched, n):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(n):
+            step(batched)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / n
 
     for _ in range(max(1, args.warmup)):
         step()
     torch.cuda.synchronize()
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(args.steps):
-        step()
-    e1.record(stream)
+    ms = timed(True, args.steps)
+    step(False)
     torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1) / args.steps
+    plain_ms = timed(False, 1)
     info = dict(w.info)
     g = info.pop("grids")
     print(json.dumps({"metric": METRIC, "value": round(w.nvis / (ms * 1e-3) / 1e6, 3), "unit": UNIT,
                       "ms_per_step": round(ms, 1), "steps": args.steps, "warmup": max(1, args.warmup),
+                      "plain": {"ms_per_step": round(plain_ms, 1),
+                                "value": round(w.nvis / (plain_ms * 1e-3) / 1e6, 3),
+                                "batched_speedup": round(plain_ms / ms, 3)},
+                      "schedule": tuned.describe(),
                       "config": {"workload": f"uneven BDA: {w.nfacets} Voronoi facets (grids {min(g)}..{max(g)}), "
                                              f"{w.nrow} rows x {w.nchan} ch x 4 corr ({w.nvis/1e6:.1f} Mvis), "
                                              f"{info['nblocks']} BDA blocks, per-vis Jones", **info,
@@ -551,17 +677,23 @@ def run_reference(args):
     if not ref.available():
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref not built (oracle/build_ref.sh)"}))
         return
+    wl = args.workload if args.workload in WORKLOADS else "combined_at_scale"
     vals = []
     cores = sample = None
+    t0 = time.perf_counter()
     for _ in range(max(1, args.steps)):
-        mv, cores, sample = cpu_reference(81)
+        mv, cores, sample = cpu_reference(wl)
         vals.append(mv)
+    wall = time.perf_counter() - t0
     v = float(np.median(vals))
+    p = WORKLOADS[wl]
     out = {"metric": METRIC, "value": round(v, 4), "unit": UNIT, "n_gpus": int(os.environ.get("WORLD_SIZE", "1")),
-           "steps": args.steps, "warmup": 0, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
-           "vs_baseline": None, "dtype": "c64 grid / f64 internal", "data": "synthetic (seeded)",
-           "config": {"workload": "multi-facet DDE (81 facets x 735^2, 232 Mvis x 4 corr, per-vis Jones), "
-                                  "reference CPU gridder+degridder on a row sample"},
+           "steps": args.steps, "warmup": 0, "ms_per_step": round(wall / max(1, args.steps) * 1e3, 1),
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c64 grid / f64 internal",
+           "data": "synthetic (seeded)",
+           "config": {"workload": f"{wl}: {p['side']}x{p['side']} facets, {p['nchan']} ch x 4 corr, per-vis Jones, "
+                                  f"{p['nw']} w-planes; reference CPU gridder+degridder on a row sample of one "
+                                  "chunk, extrapolated to the chunk"},
            "impl": "reference",
            "cpu_baseline": {"value": round(v, 4), "unit": UNIT, "cores": cores, "kind": "reference",
                             "sample": sample},
@@ -577,9 +709,11 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--scale", type=float, default=1.0)
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
-    ap.add_argument("--plain", action="store_true", help="also time the one-facet-per-launch direct path")
-    ap.add_argument("--workload", default="multifacet_dde", choices=["multifacet_dde", "uneven_bda"],
-                    help="uneven_bda: an additional workload (Voronoi facets, averaged blocks)")
+    ap.add_argument("--no-compensation", action="store_true", help="plain float32 grid sums")
+    ap.add_argument("--no-diff", action="store_true", help="skip the differentiation timing")
+    ap.add_argument("--retune", action="store_true", help="ignore the autotuner's cache")
+    ap.add_argument("--workload", default="combined_at_scale",
+                    choices=["combined_at_scale", "multifacet_dde", "uneven_bda"])
 
     args = ap.parse_args()
     if args.impl == "reference":

@@ -110,6 +110,7 @@ SIGNATURES = {
     "ddfg_degrid_batched": (C.c_int, [C.POINTER(VisSet), C.POINTER(Jones), C.POINTER(Pol), C.POINTER(Facet),
                                       C.c_int, C.POINTER(Batch), _vp]),
     "ddfg_block_geometry": (C.c_int, [C.POINTER(VisSet), C.POINTER(Facet), C.c_int, _vp, _vp]),
+    "ddfg_jones_time_map": (C.c_int, [_vp, _i64, _vp, _vp, _i32, _vp, _vp]),
     "ddfg_check_large_blocks_workspace_size": (C.c_size_t, [_i64]),
     "ddfg_check_large_blocks": (C.c_int, [C.POINTER(VisSet), _vp, C.c_size_t, _vp]),
     "ddfg_fft_plan_create": (C.c_int, [_i32, _i32, C.POINTER(_vp)]),

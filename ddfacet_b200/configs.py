@@ -8,6 +8,10 @@ correlations gridded to Stokes I, 200 power-law point sources plus 1 mJy noise, 
 per-antenna 2x2 Jones in 5-min slots (identity + 0.1 complex Gaussian), W-projection with
 32 planes, supports from 7, oversampling 11.  Every (row, channel) is its own block (no BDA).
 
+``combined_at_scale`` is one 1-hour chunk of the 8-hour, 121-facet, 256-channel workload (1485^2
+padded grids, 64 w-planes, 1000 point sources and 20 Gaussians, per-facet Jones): 232.2 M
+visibilities x 4 correlations per chunk, the full track being eight such chunks.
+
 ``plain_small`` is the single-facet, Stokes-I, 1024^2 image case (27 antennas in a 20 km
 radius, 2 h at 10 s, 16 channels over 1.30-1.45 GHz, 8 w-planes, support 7).
 
@@ -158,6 +162,122 @@ def multifacet_dde(device=None, scale=1.0, seed=1002, nfacets_side=9, nchan=64, 
                   supports=sorted(set(int(x) for x in wts[0].Sups)), wmax=wmax, nant=64, ntimes=obs.ntimes,
                   nbl=obs.nbl)
     w.host = {"obs": obs, "wterms": wts, "tess": tess, "chan_map": chan_map}
+    if keep_host:
+        w.host["vis"] = vis.cpu().pin_memory()
+    return w
+
+
+def _gen_sky_vis_gpu(uvw_d, freqs, l, m, s, fwhm_rad, ncorr, noise_sigma, seed, dev, rows=2048, chans=32):
+    """Visibilities of point and circular Gaussian sources plus complex noise on the GPU:
+    V = sum_k S_k g_k exp(+2 pi i (u l + v m + w (n - 1)) nu / c) with g_k = exp(-2 pi^2 sigma_k^2
+    (u^2 + v^2) (nu / c)^2) (sigma = FWHM / sqrt(8 ln 2); points have FWHM 0).  The phase in turns is
+    formed in FP64 and reduced before the FP32 cos/sin; rows and channels go in blocks so the
+    [rows][sources][channels] intermediates stay near 1 GB."""
+    nrow = uvw_d.shape[0]
+    nchan = len(freqs)
+    out = torch.empty((nrow, nchan, ncorr), dtype=torch.complex64, device=dev)
+    g = torch.Generator(device=dev)
+    g.manual_seed(seed)
+    lt = torch.tensor(l, dtype=torch.float64, device=dev)
+    mt = torch.tensor(m, dtype=torch.float64, device=dev)
+    lmn = torch.stack([lt, mt, torch.sqrt(1 - lt ** 2 - mt ** 2) - 1])          # [3][nsrc]
+    st = torch.tensor(s, dtype=torch.float32, device=dev)
+    sig2 = torch.tensor((np.asarray(fwhm_rad) / np.sqrt(8 * np.log(2))) ** 2, dtype=torch.float32, device=dev)
+    gauss = bool(np.any(np.asarray(fwhm_rad) > 0))
+    fr = torch.tensor(np.asarray(freqs) / C_LIGHT, dtype=torch.float64, device=dev)
+    for r0 in range(0, nrow, rows):
+        uu = uvw_d[r0:r0 + rows]
+        turns_rs = uu @ lmn                                                      # [r][s] (metres)
+        uv2 = (uu[:, 0] ** 2 + uu[:, 1] ** 2).to(torch.float32)                   # [r]
+        blk = torch.empty((uu.shape[0], nchan), dtype=torch.complex64, device=dev)
+        for c0 in range(0, nchan, chans):
+            f = fr[c0:c0 + chans]
+            t = turns_rs[:, :, None] * f[None, None, :]                             # [r][s][c]
+            frac = (t - torch.round(t)).to(torch.float32)
+            del t
+            amp = st[None, :, None].expand_as(frac)
+            if gauss:
+                amp = amp * torch.exp(-2 * np.pi ** 2 * sig2[None, :, None] * uv2[:, None, None] *
+                                      (f.to(torch.float32) ** 2)[None, None, :])
+            blk[:, c0:c0 + chans] = torch.polar(amp, 2 * np.pi * frac).sum(dim=1)
+            del frac, amp
+        noise = torch.randn((uu.shape[0], nchan, ncorr, 2), generator=g, device=dev) * noise_sigma
+        v = torch.view_as_complex(noise.contiguous())
+        v[:, :, 0] += blk
+        if ncorr > 1:
+            v[:, :, ncorr - 1] += blk
+        out[r0:r0 + rows] = v
+    return out
+
+
+def combined_at_scale(device=None, scale=1.0, seed=1005, hour=0, nfacets_side=11, nchan=256, nw=64, nsrc=1000,
+                      ngauss=20, keep_host=True):
+    """The combined at-scale workload, one 1-hour chunk of it: a 10000^2 image at 1 arcsec in 11 x 11
+    regular facets (padding 1.7: 891-pixel facets, 1485^2 padded grids, 9801^2 image), 64 antennas
+    uniform in a disk of 4 km radius (8 km across) at latitude +34 deg observing dec +40 deg for 8 h
+    at 8 s (3600 dumps, 2016 baselines), 256 channels over 0.90-1.67 GHz, 4 linear correlations
+    gridded to Stokes I, 1000 power-law point sources (0.1 mJy - 1 Jy) plus 20 circular Gaussians
+    (FWHM 5-60 arcsec) plus 1 mJy noise, per-facet per-antenna 2x2 Jones in 5-minute slots
+    (identity + 0.1 complex Gaussian, 96 slots), W-projection with 64 planes (wmax of the whole
+    8-hour track; ClassWTermModified's support rule gives support 7 at this facet size), oversampling
+    11, every (row, channel) its own block.  The chunk is hour ``hour`` (450 dumps, 907,200 rows,
+    232.2 M visibilities, 7.4 GB of visibilities); ``scale`` keeps that fraction of its dumps."""
+    dev = D._dev(device)
+    full = synth.make_observation(seed, 64, 4000.0, 34.0, 40.0, 8.0, 8.0, nchan, 0.90e9, 1.67e9)
+    wmax = float(np.max(np.abs(full.uvw[:, 2]))) * 1.001
+    nbl = full.nbl
+    d0 = hour * 450
+    d1 = d0 + max(1, int(round(450 * scale)))
+    rows = slice(d0 * nbl, d1 * nbl)
+    obs = synth.Observation(uvw=np.ascontiguousarray(full.uvw[rows]), uvw_dt=np.ascontiguousarray(full.uvw_dt[rows]),
+                            A0=full.A0[rows], A1=full.A1[rows], times=full.times[rows], freqs=full.freqs,
+                            nant=full.nant, ntimes=d1 - d0, dump_s=full.dump_s)
+    tess = geometry.regular_facets(10000, nfacets_side, 1.0, 1.7)
+    npix_pad = tess.npix_padded
+    cell = 1.0
+    wts = build_wterms(tess.facets, cell, 7, nw, wmax, npix_pad, obs.freqs, 11)
+    field_rad = tess.npix * tess.cell_rad / 2
+    l, m, s = synth.point_sky(seed + 1, nsrc, field_rad * 0.95, flux=("powerlaw", 1e-4, 1.0))
+    lg, mg, sg = synth.point_sky(seed + 6, ngauss, field_rad * 0.9, flux=("powerlaw", 1e-3, 1.0))
+    fw = np.random.default_rng(seed + 7).uniform(5.0, 60.0, ngauss) / 3600 * np.pi / 180
+    uvw_d = torch.from_numpy(obs.uvw).to(dev)
+    ncorr = 4
+    vis = _gen_sky_vis_gpu(uvw_d, obs.freqs, np.concatenate([l, lg]), np.concatenate([m, mg]),
+                           np.concatenate([s, sg]), np.concatenate([np.zeros(nsrc), fw]), ncorr, 1e-3, seed + 2, dev)
+    nrow = obs.nrow
+    flags = torch.zeros((nrow, nchan, ncorr), dtype=torch.uint8, device=dev)
+    weights = torch.ones((nrow, nchan), dtype=torch.float32, device=dev)
+    chan_map = np.zeros(nchan, np.int32)
+    bmap = _plain_map_gpu(obs.A0, obs.A1, nchan, dev)
+    vs = D.VisData.create(vis, uvw_d, flags, weights, obs.freqs, chan_map, bmap, device=dev)
+    nt = 96
+    J = synth.random_jones(seed + 3, nt, len(tess.facets), 64, 1, 0.1)
+    tmap = np.minimum(((obs.times - full.times.min()) // 300.0).astype(np.int32), nt - 1)
+    jd = D.JonesData(mode=1, kms=torch.from_numpy(J).to(dev), kms_tmap=torch.from_numpy(tmap).to(dev),
+                     kms_cmap=torch.zeros(nchan, dtype=torch.int32, device=dev),
+                     a0=torch.from_numpy(obs.A0).to(dev), a1=torch.from_numpy(obs.A1).to(dev),
+                     wavelength_mean=float(np.mean(C_LIGHT / obs.freqs)))
+    fg, fm = [], []
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(seed + 4)
+    incr = (-cell / 3600 * np.pi / 180, cell / 3600 * np.pi / 180)
+    for f, wt in zip(tess.facets, wts):
+        tabs = D.CFTables.create(wt.Wplanes, wt.WplanesConj, 11, wt.RefWave, wt.wmax, device=dev)
+        g = torch.zeros((1, 1, npix_pad, npix_pad), dtype=torch.complex64, device=dev)
+        mg = torch.view_as_complex(torch.randn((1, 1, npix_pad, npix_pad, 2), generator=gen, device=dev)) * 1e-3
+        common = dict(cf=tabs, incr=incr, cu=wt.Cu, cv=wt.Cv, l0=f.l0, m0=f.m0, idir_kms=f.index, idir_beam=0)
+        fg.append(D.FacetGrid(grid=g, sumwt=torch.zeros((1, 1), dtype=torch.float64, device=dev),
+                              sumjones=torch.zeros((2, 1), dtype=torch.float64, device=dev),
+                              sumjones_chan=torch.zeros((2, nchan), dtype=torch.float64, device=dev), **common))
+        fm.append(D.FacetGrid(grid=mg, **common))
+    pol = D.make_pol([9, 10, 11, 12], [1])
+    w = Workload("combined_at_scale", vs, fg, fm, jd, pol, nvis=nrow * nchan, nrow=nrow, nchan=nchan, ncorr=ncorr,
+                 nfacets=len(fg))
+    w.info = dict(npix=tess.npix, npix_facet=tess.npix_facet, npix_padded=npix_pad, nw=nw,
+                  supports=sorted(set(int(x) for x in wts[0].Sups)), wmax=wmax, nant=64, ntimes=obs.ntimes,
+                  nbl=nbl, chunk=f"hour {hour} of 8: dumps {d0}-{d1 - 1} of 3600", nsrc=nsrc, ngauss=ngauss,
+                  full_track_nvis=full.nrow * nchan)
+    w.host = {"obs": obs, "wterms": wts, "tess": tess, "chan_map": chan_map, "J": J, "tmap": tmap}
     if keep_host:
         w.host["vis"] = vis.cpu().pin_memory()
     return w

@@ -70,7 +70,31 @@ __global__ void large_check_kernel(const ddfg_vis vs, const unsigned int *bits, 
   }
 }
 
+// Jones time slot of every row: the last slot [t0, t1) that contains the row's time, 0 if none
+// (ClassJones.GiveTimeMapping, ClassJones.py:415-439).
+__global__ void jones_time_map_kernel(const double *times, int64_t nrow, const double *t0, const double *t1, int nt,
+                                      int32_t *out) {
+  for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < nrow; r += (int64_t)gridDim.x * blockDim.x) {
+    const double t = times[r];
+    int v = 0;
+    for (int it = 0; it < nt; ++it)
+      if (t >= t0[it] && t < t1[it]) v = it;
+    out[r] = v;
+  }
+}
+
 }  // namespace
+
+extern "C" int ddfg_jones_time_map(const double *times, int64_t nrow, const double *t0, const double *t1, int32_t nt,
+                                   int32_t *out, void *stream) {
+  if (nrow < 0 || nt < 0 || (nrow > 0 && (!times || !out)) || (nt > 0 && (!t0 || !t1)))
+    return ddfg_set_error(DDFG_EINVAL, "jones_time_map: null pointer or negative size");
+  if (nrow == 0) return DDFG_OK;
+  jones_time_map_kernel<<<ddfg_num_ctas(4), 256, 0, (cudaStream_t)stream>>>(times, nrow, t0, t1, nt, out);
+  const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return ddfg_set_error(DDFG_ECUDA, "jones_time_map: %s", cudaGetErrorString(e));
+  return DDFG_OK;
+}
 
 extern "C" int ddfg_block_geometry(const ddfg_vis *vs, const ddfg_facet *facet, int degrid_means, int32_t *out,
                                    void *stream) {

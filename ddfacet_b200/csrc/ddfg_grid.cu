@@ -269,7 +269,7 @@ int ddfg_launch_grid(const ddfg_vis *vs, const ddfg_jones *js, const ddfg_facet 
   const bool single = vs->single_vis_blocks != 0;
   const size_t budget = single ? 110 * 1024 : 74 * 1024;
   const size_t tile_bytes = (size_t)(single ? 8 : 4) * kTileCells * sizeof(float2);
-  int tiles = (nvispol == 1 && !(batch && (batch->flags & 2))) ? 1 : 0;
+  int tiles = (nvispol == 1 && batch && (batch->flags & 2)) ? 1 : 0;
   if (tiles && budget < tile_bytes + per_facet_smem) tiles = 0;
   const int max_fit = (int)((budget - (tiles ? tile_bytes : 0)) / per_facet_smem);
   if (max_fit < 1) return ddfg_set_error(DDFG_ESIZE, "grid: too many bands/channels for the shared accumulators");

@@ -90,17 +90,22 @@ __device__ __forceinline__ int stage_pack(const FacetTable &tab, const Sched &sc
 // the atomic returns the old value a, the cell now holds fl(a + v), and TwoSum(a, v) recovers
 // fl(a + v) - (a + v) exactly (Knuth, TAOCP vol. 2, 4.2.2).  Summed over a call, hi + lo is the
 // exact sum of the addends up to the (second-order) rounding of lo's own additions.
+// fl(a + v) - (a + v), componentwise, exactly (TwoSum).
+__device__ __forceinline__ float2 two_sum_err(float2 a, float2 v) {
+  const float sx = __fadd_rn(a.x, v.x), sy = __fadd_rn(a.y, v.y);
+  const float bx = __fsub_rn(sx, a.x), by = __fsub_rn(sy, a.y);
+  return make_float2(__fadd_rn(__fsub_rn(a.x, __fsub_rn(sx, bx)), __fsub_rn(v.x, bx)),
+                     __fadd_rn(__fsub_rn(a.y, __fsub_rn(sy, by)), __fsub_rn(v.y, by)));
+}
+
 __device__ __forceinline__ void comp_add(float2 *cell, ptrdiff_t lo_off, float2 v) {
   float2 a;
   asm volatile("atom.global.v2.f32.add {%0, %1}, [%2], {%3, %4};"
                : "=f"(a.x), "=f"(a.y)
                : "l"(cell), "f"(v.x), "f"(v.y)
                : "memory");
-  const float sx = __fadd_rn(a.x, v.x), sy = __fadd_rn(a.y, v.y);
-  const float bx = __fsub_rn(sx, a.x), by = __fsub_rn(sy, a.y);
-  const float ex = __fadd_rn(__fsub_rn(a.x, __fsub_rn(sx, bx)), __fsub_rn(v.x, bx));
-  const float ey = __fadd_rn(__fsub_rn(a.y, __fsub_rn(sy, by)), __fsub_rn(v.y, by));
-  if (ex != 0.f || ey != 0.f) red_add(cell + lo_off, make_float2(ex, ey));
+  const float2 e = two_sum_err(a, v);
+  if (e.x != 0.f || e.y != 0.f) red_add(cell + lo_off, e);
 }
 
 __device__ __forceinline__ void grid_add(float2 *cell, bool comp, ptrdiff_t lo_off, float2 v) {
@@ -288,7 +293,9 @@ __device__ __forceinline__ void scatter_q(const GridRecord<NPOL> &rec, const ddf
 // and a __syncwarp orders one record's updates before the next's -- and then adds every touched
 // tile cell to the grid once.  The grid sees one addition per touched cell instead of one per tap
 // (S^2 per record), which also makes the compensated additions cheap.
-constexpr int kTileW = 32, kTileH = 32, kTilePitch = 33;  // cells; the odd pitch spreads rows over banks
+// Pitch 39 = 7 (mod 16): with 8-byte cells a 128-byte shared-memory wavefront holds 16 cells, and
+// the rows of a 7 x 7 footprint (lanes 0-6 row 0, 7-13 row 1, ...) then fall on distinct banks.
+constexpr int kTileW = 32, kTileH = 32, kTilePitch = 39;
 constexpr int kTileCells = kTileH * kTilePitch;
 
 // Lays the warp's records onto facet f through the warp's tile; returns false (having done
@@ -312,8 +319,13 @@ __device__ __forceinline__ bool scatter_tile(const GridRecord<1> &rec, const ddf
   const int y1 = __reduce_max_sync(0xffffffffu, rec.valid ? rec.g.locy - sup : -1);
   const int bw = x1 - x0 + S0, bh = y1 - y0 + S0;
   if (bw > kTileW || bh > kTileH) return false;
-  for (int r = 0; r < bh; ++r)
-    if (lane < bw) tile[r * kTilePitch + lane] = czero();
+  // the bbox's cells lane-strided over all 32 lanes: cell i is row i / bw, column i % bw
+  const int ncell = bw * bh;
+  const unsigned inv_bw = (65536u + (unsigned)bw - 1u) / (unsigned)bw;  // i / bw == (i * inv_bw) >> 16, i < 1024
+  for (int i = lane; i < ncell; i += 32) {
+    const int r = (int)(((unsigned)i * inv_bw) >> 16);
+    tile[r * kTilePitch + (i - r * bw)] = czero();
+  }
   const int s_inv0 = S0 | (int)(((65536u + (unsigned)S0 - 1u) / (unsigned)S0) << 8);
   ltt.set(s_inv0, kTilePitch, lane);
   const float2 *cf_lane = (const float2 *)f.cf_data + lane;
@@ -367,10 +379,44 @@ __device__ __forceinline__ bool scatter_tile(const GridRecord<1> &rec, const ddf
   float2 *gbase = (float2 *)f.grid + ((size_t)(g0 * f.npol) * f.ny + y0) * f.nx + x0;
   const bool comp = f.grid_lo != nullptr;
   const ptrdiff_t lo_off = comp ? (float2 *)f.grid_lo - (float2 *)f.grid : 0;
-  for (int r = 0; r < bh; ++r) {
-    if (lane < bw) {
-      const float2 v = tile[r * kTilePitch + lane];
-      if (v.x != 0.f || v.y != 0.f) grid_add(gbase + (size_t)r * f.nx + lane, comp, lo_off, v);
+  if (comp) {
+    // four cells per lane at a time, so four returning atomics are in flight before their TwoSums
+    for (int i0 = lane; i0 < ncell; i0 += 128) {
+      float2 v[4], a[4];
+      float2 *cell[4];
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        const int i = i0 + 32 * k;
+        v[k] = czero();
+        cell[k] = gbase;
+        if (i < ncell) {
+          const int r = (int)(((unsigned)i * inv_bw) >> 16), c = i - r * bw;
+          v[k] = tile[r * kTilePitch + c];
+          cell[k] = gbase + (size_t)r * f.nx + c;
+        }
+      }
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        a[k] = czero();
+        if (v[k].x != 0.f || v[k].y != 0.f)
+          asm volatile("atom.global.v2.f32.add {%0, %1}, [%2], {%3, %4};"
+                       : "=f"(a[k].x), "=f"(a[k].y)
+                       : "l"(cell[k]), "f"(v[k].x), "f"(v[k].y)
+                       : "memory");
+      }
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        if (v[k].x != 0.f || v[k].y != 0.f) {
+          const float2 e = two_sum_err(a[k], v[k]);
+          if (e.x != 0.f || e.y != 0.f) red_add(cell[k] + lo_off, e);
+        }
+      }
+    }
+  } else {
+    for (int i = lane; i < ncell; i += 32) {
+      const int r = (int)(((unsigned)i * inv_bw) >> 16), c = i - r * bw;
+      const float2 v = tile[r * kTilePitch + c];
+      if (v.x != 0.f || v.y != 0.f) red_add(gbase + (size_t)r * f.nx + c, v);
     }
   }
   __syncwarp();

@@ -363,14 +363,14 @@ def make_pol(corr_ids, stokes_ids) -> _abi.Pol:
 class Batch:
     """Scheduling of the batched (persistent, queue-driven) calls and their workspace
     (ddfg_batch): facets per pack, stripes per queue item, resident CTAs per SM (0 = library
-    default); ``static`` replaces the queue by a fixed item order and ``no_tiles`` turns off the
-    warps' grid tiles (both for measurements)."""
+    default); ``static`` replaces the queue by a fixed item order (for measurements) and ``tiles``
+    has the gridder's warps sum each stripe in a shared-memory tile before adding it to the grid."""
     workspace: torch.Tensor
     facets_per_pack: int = 0
     stripes_per_item: int = 0
     ctas_per_sm: int = 0
     static: bool = False
-    no_tiles: bool = False
+    tiles: bool = False
 
     @classmethod
     def create(cls, device=None, **kw) -> "Batch":
@@ -385,12 +385,12 @@ class Batch:
         b.facets_per_pack = int(self.facets_per_pack)
         b.stripes_per_item = int(self.stripes_per_item)
         b.ctas_per_sm = int(self.ctas_per_sm)
-        b.flags = (1 if self.static else 0) | (2 if self.no_tiles else 0)
+        b.flags = (1 if self.static else 0) | (2 if self.tiles else 0)
         return b
 
     def describe(self) -> dict:
         return {"facets_per_pack": int(self.facets_per_pack), "stripes_per_item": int(self.stripes_per_item),
-                "ctas_per_sm": int(self.ctas_per_sm), "queue": not self.static, "tiles": not self.no_tiles}
+                "ctas_per_sm": int(self.ctas_per_sm), "queue": not self.static, "tiles": bool(self.tiles)}
 
 
 def grid(vs: VisData, facets: List[FacetGrid], pol: _abi.Pol, jones: Optional[JonesData] = None, dopsf=False,

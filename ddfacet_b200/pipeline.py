@@ -43,14 +43,17 @@ class PipelinedStep:
 
     ``run(host)`` takes pinned host tensors ``vis`` (complex64 [nrow][nchan][ncorr]), ``uvw``,
     ``flags``, ``weights`` and ``out`` (complex64, receives the residual visibilities) and
-    returns when the copies are queued; the caller synchronises."""
+    returns when the copies are queued; the caller synchronises.  With ``batch_grid`` /
+    ``batch_degrid`` the chunks go through the batched (queue-driven) calls."""
 
     def __init__(self, chunks: Sequence[Chunk], facets_grid: List[D.FacetGrid], facets_model: List[D.FacetGrid],
-                 pol, device=None):
+                 pol, device=None, batch_grid: Optional[D.Batch] = None, batch_degrid: Optional[D.Batch] = None):
         self.chunks = list(chunks)
         self.facets_grid = facets_grid
         self.facets_model = facets_model
         self.pol = pol
+        self.batch_grid = batch_grid
+        self.batch_degrid = batch_degrid
         dev = D._dev(device)
         self.h2d = torch.cuda.Stream(device=dev)
         self.d2h = torch.cuda.Stream(device=dev)
@@ -71,8 +74,8 @@ class PipelinedStep:
                 loaded.append(ev)
         for c, ev in zip(self.chunks, loaded):
             comp.wait_event(ev)
-            D.degrid(c.vs, self.facets_model, self.pol, c.jones, stream=comp)
-            D.grid(c.vs, self.facets_grid, self.pol, c.jones, stream=comp)
+            D.degrid(c.vs, self.facets_model, self.pol, c.jones, stream=comp, batch=self.batch_degrid)
+            D.grid(c.vs, self.facets_grid, self.pol, c.jones, stream=comp, batch=self.batch_grid)
             e = torch.cuda.Event()
             e.record(comp)
             done.append(e)

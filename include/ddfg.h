@@ -153,8 +153,10 @@ typedef struct ddfg_batch {
   int32_t facets_per_pack;     /* facets applied to a stripe before the next stripe (0: default) */
   int32_t stripes_per_item;    /* stripes of one queue item (0: default)                   */
   int32_t ctas_per_sm;         /* resident CTAs per SM of the persistent launch (0: occupancy) */
-  int32_t flags;               /* bit 0: static item order instead of the queue; bit 1: no warp
-                                  grid tiles (direct tap additions) -- both for measurements */
+  int32_t flags;               /* bit 0: static item order instead of the queue (for
+                                  measurements); bit 1: the gridder's warps sum each stripe into a
+                                  shared-memory tile and add the touched cells to the grid once
+                                  (one Stokes plane; pays when a stripe's footprints overlap) */
 } ddfg_batch;
 
 /* Library and device checks. */
@@ -302,6 +304,13 @@ int ddfg_degrid_batched(const ddfg_vis *vs, const ddfg_jones *js, const ddfg_pol
  * step on.  Uses the kernels' own index code.  A check entry point: the reference exposes these
  * indices only inside its loops. */
 int ddfg_block_geometry(const ddfg_vis *vs, const ddfg_facet *facet, int degrid_means, int32_t *out, void *stream);
+
+/* Jones time slot of every row (ClassJones.GiveTimeMapping, DDFacet/Data/ClassJones.py:415-439):
+ * out[r] = the last it with t0[it] <= times[r] < t1[it], 0 when no slot contains the row; the times
+ * need not be sorted.  times float64 [nrow]; t0, t1 float64 [nt] (the solutions' slot bounds);
+ * out int32 [nrow] (LJones[1] / LJones[3], the time maps ddfg_jones.kms_tmap / beam_tmap take). */
+int ddfg_jones_time_map(const double *times, int64_t nrow, const double *t0, const double *t1, int32_t nt,
+                        int32_t *out, void *stream);
 
 /* Bytes of device scratch ddfg_check_large_blocks needs. */
 size_t ddfg_check_large_blocks_workspace_size(int64_t nblocks);

@@ -18,7 +18,11 @@ The reference's Python modules are imported with stand-ins for the absent option
                    pyAccumulateWeightsOntoGridNoSem, the Briggs step and
                    ClassVisServer._finalizeWeights_handler on a small observation
 
-    python tests/golden/make_golden.py [/path/to/reference] [--only weights]
+  maps_golden.npz  ClassJones.GiveTimeMapping / GiveVisToJonesChanMapping and the channel maps
+                   ClassVisServer.Init builds (grid bands, channels within bands, degridding bands)
+                   for two measurement sets under three frequency settings
+
+    python tests/golden/make_golden.py [/path/to/reference] [--only weights|maps]
 """
 import os
 import sys
@@ -28,8 +32,10 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
-_args = [a for a in sys.argv[1:] if not a.startswith("--") and a != "weights"]
-REF = _args[0] if _args else "/root/reference"
+_args = [a for a in sys.argv[1:] if not a.startswith("--") and a not in ("weights", "maps")]
+REF = _args[0] if _args else os.environ.get("DDFACET_REF", "")
+if not REF or not os.path.isdir(REF):
+    sys.exit("usage: make_golden.py <reference checkout> (or set DDFACET_REF)")
 ONLY = sys.argv[sys.argv.index("--only") + 1] if "--only" in sys.argv else None
 
 
@@ -201,10 +207,86 @@ def make_weights_golden():
     print("weights golden written")
 
 
+class _FakeMS:
+    """The measurement-set object ClassVisServer.Init reads: channel frequencies and widths, and the
+    few methods its loop calls (no table is opened)."""
+    SPECS = {}
+
+    def __init__(self, msname, **kw):
+        self.MSName = msname
+        self.ChanFreq, self.ChanWidth = self.SPECS[msname]
+        self.empty = False
+        self.Ncorr = 4
+        self.CorrelationIds = [9, 10, 11, 12]
+        self.maincache = types.SimpleNamespace(dirname="/tmp")
+
+    def getPerChunkRowCounts(self):
+        return [100]
+
+    def get_obs_details(self):
+        return {}
+
+    def numChunks(self):
+        return 1
+
+    def __str__(self):
+        return self.MSName
+
+
+def make_maps_golden():
+    V, _ = import_visserver()
+    from DDFacet.Data import ClassJones as CJ
+
+    rng = np.random.default_rng(41)
+    out = {}
+    # ---- Jones time map: unsorted times, a gap between slots, an overlap, rows outside every slot
+    times = rng.uniform(-100.0, 3700.0, 6000)
+    t0 = np.array([0.0, 300.0, 600.0, 900.0, 1300.0, 1600.0, 1800.0, 2400.0, 3000.0])
+    t1 = np.array([300.0, 600.0, 900.0, 1200.0, 1600.0, 1900.0, 2100.0, 3000.0, 3600.0])
+    sols = {"Jones": np.zeros((t0.size, 1, 1, 1, 2, 2), np.complex64), "t0": t0, "t1": t1}
+    out.update(times=times, t0=t0, t1=t1, time_map=CJ.ClassJones.GiveTimeMapping(None, sols, times))
+    # ---- visibility channel -> Jones channel
+    freqs = np.linspace(1.30e9, 1.45e9, 16)
+    doms = np.array([[1.28e9, 1.33e9], [1.33e9, 1.38e9], [1.38e9, 1.43e9], [1.43e9, 1.48e9]])
+    fake = types.SimpleNamespace(MS=types.SimpleNamespace(ChanFreq=freqs, NSPWChan=freqs.size))
+    out.update(jchan_freqs=freqs, jchan_domains=doms, jchan_map=CJ.ClassJones.GiveVisToJonesChanMapping(fake, doms))
+    # ---- grid / degrid channel maps of two measurement sets (ClassVisServer.Init)
+    f1 = np.linspace(1.30e9, 1.45e9, 16)
+    f2 = np.linspace(1.40e9, 1.62e9, 8)
+    _FakeMS.SPECS = {"a.ms": (f1, np.full(16, f1[1] - f1[0])), "b.ms": (f2, np.full(8, f2[1] - f2[0]))}
+    out.update(ms_a_freq=f1, ms_a_width=_FakeMS.SPECS["a.ms"][1], ms_b_freq=f2, ms_b_width=_FakeMS.SPECS["b.ms"][1])
+    V.ClassMS = types.SimpleNamespace(ClassMS=_FakeMS)
+    settings = [(0.0, 3, 0.0, 0), (40.0, 1, 25.0, 0), (0.0, 1, 0.0, 4), (100.0, 2, 0.0, 3)]
+    for k, (band_mhz, nband, dband_mhz, ndband) in enumerate(settings):
+        vs = V.ClassVisServer.__new__(V.ClassVisServer)
+        vs.GD = {"Data": {"Dask": False, "MS": "a.ms"}, "Cache": {"Reset": 0, "Dir": ""},
+                 "Freq": {"BandMHz": band_mhz, "NBand": nband, "DegridBandMHz": dband_mhz, "NDegridBand": ndband},
+                 "RIME": {"PolMode": "I"}, "HMP": {"Alpha": [0., 0., 1.]}, "SSDClean": {"SSDSolvePars": ["S", "Alpha"]}}
+        vs.MSList = ["a.ms", "b.ms"]
+        vs.DicoSelectOptions = {"DDID": 0, "Field": 0}
+        vs.ColName, vs.SubColName, vs.TaQL, vs.TMemChunkSize, vs.DATA = "DATA", None, None, 1.0, None
+        V.ClassVisServer.Init(vs)
+        out[f"s{k}_settings"] = np.array([band_mhz, nband, dband_mhz, ndband], np.float64)
+        out[f"s{k}_nbands"] = np.array(vs.NFreqBands)
+        out[f"s{k}_centers"] = np.asarray(vs.FreqBandCenters)
+        for ims in (0, 1):
+            out[f"s{k}_ms{ims}_map"] = np.asarray(vs.DicoMSChanMapping[ims])
+            out[f"s{k}_ms{ims}_mapchan"] = np.asarray(vs.DicoMSChanMappingChan[ims])
+            out[f"s{k}_ms{ims}_degrid"] = np.asarray(vs.DicoMSChanMappingDegridding[ims])
+            out[f"s{k}_ms{ims}_degrid_freqs"] = np.asarray(vs.FreqBandChannelsDegrid[ims])
+    out["nsettings"] = np.array(len(settings))
+    np.savez_compressed(os.path.join(HERE, "maps_golden.npz"), **out)
+    print("maps golden written")
+
+
 def main():
     if ONLY == "weights":
         import_reference()
         make_weights_golden()
+        return
+    if ONLY == "maps":
+        import_reference()
+        make_maps_golden()
         return
     ModCF, SM, ModFFTW = import_reference()
     sys.path.insert(0, ROOT)

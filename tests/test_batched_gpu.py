@@ -37,7 +37,8 @@ def _case(name):
 
 
 @pytest.mark.parametrize("name", ["single", "bda1_jones", "bda2_blockjones", "iquv"])
-@pytest.mark.parametrize("batch_kw", [{}, {"stripes_per_item": 1, "ctas_per_sm": 1}, {"static": True}])
+@pytest.mark.parametrize("batch_kw", [{}, {"stripes_per_item": 1, "ctas_per_sm": 1}, {"static": True},
+                                      {"tiles": True}, {"tiles": True, "stripes_per_item": 2}])
 def test_batched_against_reference(name, batch_kw):
     c = _case(name)
     r = cases.run_ref_grid(c)
@@ -78,7 +79,8 @@ def test_batched_large_block_items():
 
 
 @pytest.mark.parametrize("batch_kw", [{}, {"facets_per_pack": 3}, {"facets_per_pack": 1, "stripes_per_item": 3},
-                                      {"facets_per_pack": 7, "static": True}, {"ctas_per_sm": 1}])
+                                      {"facets_per_pack": 7, "static": True}, {"ctas_per_sm": 1},
+                                      {"tiles": True, "facets_per_pack": 5}])
 def test_batched_uneven_facets(batch_kw):
     """20 facets of four grid sizes in one batched grid and one batched degrid call, each against
     the reference on that facet alone, under several schedules."""
@@ -108,13 +110,14 @@ def test_batched_uneven_facets(batch_kw):
     assert cases.rel_rms(vis0 - got, vis0 - want) < TOL
 
 
-@pytest.mark.parametrize("batched", [False, True])
-def test_compensated_grid(batched):
-    c = cases.make_case(ncorr=4, stokes_ids=(1, 2), nw=3, ntimes=120, nant=16, lm=(0.004, 0.002))
+@pytest.mark.parametrize("batched,stokes,tiles", [(False, (1, 2), False), (True, (1, 2), False), (True, (1,), True)])
+def test_compensated_grid(batched, stokes, tiles):
+    c = cases.make_case(ncorr=4, stokes_ids=stokes, nw=3, ntimes=120, nant=16, lm=(0.004, 0.002))
     f64 = cases.run_fp64_grid(c)["grid"]
     r = cases.run_ref_grid(c)["grid"]
-    plain = cases.run_gpu_grid(c, batched=batched)
-    comp = cases.run_gpu_grid(c, batched=batched, compensated=True)
+    kw = {"tiles": True} if tiles else None
+    plain = cases.run_gpu_grid(c, batched=batched, batch_kw=kw)
+    comp = cases.run_gpu_grid(c, batched=batched, compensated=True, batch_kw=kw)
     e_plain, e_comp = cases.rel_rms(plain["grid"], f64), cases.rel_rms(comp["grid"], f64)
     print(f"rel RMS vs FP64: plain {e_plain:.2e}, compensated {e_comp:.2e}, reference {cases.rel_rms(r, f64):.2e}")
     assert cases.rel_rms(comp["grid"], r) < TOL

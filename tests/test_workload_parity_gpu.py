@@ -83,7 +83,7 @@ def test_workload_grid_against_reference_and_fp64(small):
         f.grid.zero_()
         f.sumwt.zero_()
         f.with_compensation()
-    D.grid(w.vs, w.facets_grid, w.pol, w.jones, batch=D.Batch.create(w.vs.vis.device))
+    D.grid(w.vs, w.facets_grid, w.pol, w.jones, batch=D.Batch.create(w.vs.vis.device, tiles=True))
     torch.cuda.synchronize()
     for fi in PICK:
         c = _case(w, fi, host["vis"], host)
@@ -170,7 +170,7 @@ def test_full_depth_compensated_vs_fp64():
             f.grid_lo = None
             if comp:
                 f.with_compensation()
-        D.grid(w.vs, fs, w.pol, w.jones, batch=D.Batch.create(w.vs.vis.device))
+        D.grid(w.vs, fs, w.pol, w.jones, batch=D.Batch.create(w.vs.vis.device, tiles=comp))
         torch.cuda.synchronize()
         errs[comp] = [fs[i].grid.cpu().numpy() for i in range(len(pick))]
     for i, fi in enumerate(pick):
