@@ -104,6 +104,9 @@ SIGNATURES = {
     "ddfg_bda_mode1_count": (C.c_int, [_vp, _vp, _vp, _i32, _i32, _vp, _f64, _f64, _f64, _f64, _vp, _vp, _vp]),
     "ddfg_bda_mode1_write": (C.c_int, [_vp, _vp, _vp, _i32, _i32, _vp, _f64, _f64, _f64, _f64, _vp, _vp, _vp, _vp,
                                        _vp]),
+    "ddfg_bda_mode2_count": (C.c_int, [_vp, _vp, _vp, _i32, _i32, _vp, _f64, _f64, _f64, _f64, _vp, _vp, _vp]),
+    "ddfg_bda_mode2_write": (C.c_int, [_vp, _vp, _vp, _i32, _i32, _vp, _f64, _f64, _f64, _f64, _vp, _vp, _vp, _vp,
+                                       _vp]),
     "ddfg_batch_workspace_size": (C.c_size_t, []),
     "ddfg_grid_batched": (C.c_int, [C.POINTER(VisSet), C.POINTER(Jones), C.POINTER(Pol), C.POINTER(Facet), C.c_int,
                                     C.c_int, C.POINTER(Batch), _vp]),

@@ -78,9 +78,13 @@ class Tuned:
     cached: bool = False
 
     def describe(self) -> dict:
+        def short(c):
+            return "fpp%d/spi%d%s" % (c.get("facets_per_pack", 0), c.get("stripes_per_item", 0),
+                                      "/tiles" if c.get("tiles") else "")
+
         return {"grid": self.grid.describe(), "degrid": self.degrid.describe(), "cached": self.cached,
                 "sample_grid_ms": round(self.grid_ms, 3), "sample_degrid_ms": round(self.degrid_ms, 3),
-                "candidates": {k: len(v) for k, v in self.table.items()}}
+                "timed_ms": {k: {short(c): ms for c, ms in v} for k, v in self.table.items()}}
 
 
 def tune(vs: D.VisData, facets_grid: Sequence[D.FacetGrid], facets_model: Sequence[D.FacetGrid], pol,

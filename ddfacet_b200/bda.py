@@ -215,10 +215,11 @@ def plain_map(A0, A1, nchan, uvw=None):
     return m
 
 
-def smear_mapping_gpu(A0, A1, uvw, freqs, dfreq, dPhi, l, chan_map, device=None):
-    """Mode-1 map (``GiveBlocksRowsListBL_old`` for every baseline, packed as
-    ``collectSmearMapping`` does) built on the GPU by ddfg_bda_mode1_count / _write: the same
-    words as ``smear_mapping(..., mode=1)``.  Returns an int32 device tensor."""
+def smear_mapping_gpu(A0, A1, uvw, freqs, dfreq, dPhi, l, chan_map, device=None, mode=1):
+    """The block map of every baseline, packed as ``collectSmearMapping`` does, built on the GPU:
+    mode 1 (``GiveBlocksRowsListBL_old``, ddfg_bda_mode1_count / _write) or mode 2
+    (``GiveBlocksRowsListBL``, ddfg_bda_mode2_count / _write, ``l`` being l_max): the same words as
+    ``smear_mapping(..., mode=mode)``.  Returns an int32 device tensor."""
     from . import _abi, device as D
 
     dev = D._dev(device)
@@ -252,15 +253,19 @@ def smear_mapping_gpu(A0, A1, uvw, freqs, dfreq, dPhi, l, chan_map, device=None)
     nu0 = float(np.max(freqs))
     args = (uvw_d.data_ptr(), rows.data_ptr(), bl_off.data_ptr(), nbl, nchan, cmap.data_ptr(), float(dfreq),
             float(dPhi), float(l), nu0)
-    _abi.check(lib.ddfg_bda_mode1_count(*args, nblk.data_ptr(), nwords.data_ptr(), st))
+    count, write = ((lib.ddfg_bda_mode1_count, lib.ddfg_bda_mode1_write) if mode == 1 else
+                    (lib.ddfg_bda_mode2_count, lib.ddfg_bda_mode2_write))
+    _abi.check(count(*args, nblk.data_ptr(), nwords.data_ptr(), st))
+    if mode != 1 and bool((nblk[:nbl] < 0).any()):
+        raise IndexError("BDA mode 2: a baseline has a single row (GiveBlocksRowsListBL reads the row "
+                         "difference before the last)")
     blk_off = torch.cumsum(nblk, 0) - nblk
     word_off = torch.cumsum(nwords, 0) - nwords
     nb = int(nblk[:nbl].sum().item())
     nw = int(nwords[:nbl].sum().item())
     m = torch.empty(2 + nb + nw, dtype=torch.int32, device=dev)
     m[0:2] = torch.from_numpy(_header(nb)).to(dev)
-    _abi.check(lib.ddfg_bda_mode1_write(*args, blk_off.data_ptr(), word_off.data_ptr(), m[2:].data_ptr(),
-                                        m[2 + nb:].data_ptr(), st))
+    _abi.check(write(*args, blk_off.data_ptr(), word_off.data_ptr(), m[2:].data_ptr(), m[2 + nb:].data_ptr(), st))
     return m
 
 

@@ -111,7 +111,7 @@ def build_wterms(tess_facets, cell, sup, nw, wmax, npix, freqs, overs, threads=8
 
 
 def multifacet_dde(device=None, scale=1.0, seed=1002, nfacets_side=9, nchan=64, nw=32, with_jones=True,
-                   keep_host=True, nsrc=200):
+                   keep_host=True, nsrc=200, jones_sigma=0.1):
     dev = D._dev(device)
     hours = 4.0 * scale
     obs = synth.make_observation(seed, 64, 4000.0, 34.0, 40.0, hours, 8.0, nchan, 0.90e9, 1.67e9)
@@ -135,7 +135,7 @@ def multifacet_dde(device=None, scale=1.0, seed=1002, nfacets_side=9, nchan=64, 
     jd = None
     if with_jones:
         nt = int(np.ceil(hours * 3600 / 300.0))
-        J = synth.random_jones(seed + 3, nt, len(tess.facets), 64, 1, 0.1)
+        J = synth.random_jones(seed + 3, nt, len(tess.facets), 64, 1, jones_sigma)
         tmap = np.minimum(((obs.times - obs.times.min()) // 300.0).astype(np.int32), nt - 1)
         jd = D.JonesData(mode=1, kms=torch.from_numpy(J).to(dev), kms_tmap=torch.from_numpy(tmap).to(dev),
                          kms_cmap=torch.zeros(nchan, dtype=torch.int32, device=dev),

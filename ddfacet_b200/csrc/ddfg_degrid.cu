@@ -233,6 +233,7 @@ int ddfg_launch_degrid(const ddfg_vis *vs, const ddfg_jones *js, const ddfg_face
     sc.npacks = 1;
     sc.max_pack = n;
     sc.acc_stride = 0;
+    sc.small_stride = 0;
     sc.tiles = 0;
     sc.nstripes = nstripes;
     const long long spi = (batch && batch->stripes_per_item > 0) ? batch->stripes_per_item

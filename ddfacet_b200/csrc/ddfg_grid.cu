@@ -40,22 +40,28 @@ __device__ __forceinline__ void scatter_any(const GridRecord<NPOL> &rec, const d
   scatter_q<NPOL, SLOTS>(rec, f, npol_used, lt, lane);
 }
 
-// Adds the CTA's shared sums of the pack's npk facets to their float64 outputs.
-__device__ __forceinline__ void flush_grid_sums(const ddfg_facet *sf, int npk, const double *s_acc, int acc_stride,
+// Adds the CTA's shared sums of the pack's npk facets to their float64 outputs.  Each facet's
+// accumulators are one copy of the weight and Jones sums per warp (updated by that warp alone, so
+// its lanes never contend with other warps for them), then the per-channel Jones sums.
+__device__ __forceinline__ void flush_grid_sums(const ddfg_facet *sf, int npk, const double *s_acc, const Sched &sc,
                                                 const ddfg_jones &js, int nchan) {
+  const int nwarps = blockDim.x >> 5;
   for (int fi = 0; fi < npk; ++fi) {
     const ddfg_facet &f = sf[fi];
-    const double *a = s_acc + (size_t)fi * acc_stride;
+    const double *a = s_acc + (size_t)fi * sc.acc_stride;
+    const double *a_chan = a + nwarps * sc.small_stride;
     const int nsw = f.nband * f.npol;
-    for (int i = threadIdx.x; i < nsw; i += blockDim.x)
-      if (f.sumwt && a[i] != 0.) atomicAdd(&f.sumwt[i], a[i]);
-    if (js.mode != 0) {
-      for (int i = threadIdx.x; i < 2 * f.nband; i += blockDim.x)
-        if (f.sumjones && a[nsw + i] != 0.) atomicAdd(&f.sumjones[i], a[nsw + i]);
-      for (int i = threadIdx.x; i < 2 * nchan; i += blockDim.x)
-        if (f.sumjones_chan && a[nsw + 2 * f.nband + i] != 0.)
-          atomicAdd(&f.sumjones_chan[i], a[nsw + 2 * f.nband + i]);
+    const int nsmall = nsw + (js.mode != 0 ? 2 * f.nband : 0);
+    for (int i = threadIdx.x; i < nsmall; i += blockDim.x) {
+      double v = 0.;
+      for (int w = 0; w < nwarps; ++w) v += a[w * sc.small_stride + i];
+      double *dst = i < nsw ? f.sumwt + i : (f.sumjones ? f.sumjones + (i - nsw) : nullptr);
+      if (i < nsw && !f.sumwt) dst = nullptr;
+      if (dst && v != 0.) atomicAdd(dst, v);
     }
+    if (js.mode != 0)
+      for (int i = threadIdx.x; i < 2 * nchan; i += blockDim.x)
+        if (f.sumjones_chan && a_chan[i] != 0.) atomicAdd(&f.sumjones_chan[i], a_chan[i]);
   }
 }
 
@@ -65,7 +71,7 @@ __device__ __forceinline__ void enter_pack(const FacetTable &tab, const Sched &s
                                            int pack, int &cur, int &npk, ddfg_facet *sf, double *s_n0m1,
                                            double *s_acc) {
   if (pack == cur) return;
-  if (cur >= 0) flush_grid_sums(sf, npk, s_acc, sc.acc_stride, js, nchan);
+  if (cur >= 0) flush_grid_sums(sf, npk, s_acc, sc, js, nchan);
   __syncthreads();
   npk = stage_pack(tab, sc, pack, sf, s_n0m1);
   for (int i = threadIdx.x; i < npk * sc.acc_stride; i += blockDim.x) s_acc[i] = 0.;
@@ -109,16 +115,16 @@ __global__ void __launch_bounds__(256) grid_single_q(const ddfg_vis vs, const dd
       for (int fi = 0; fi < npk; ++fi) {
         const ddfg_facet &f = sf[fi];
         const int npol_used = min(gp.nvispol, f.npol);
-        double *a = s_acc + (size_t)fi * sc.acc_stride;
-        double *a_sumj = a + f.nband * f.npol;
+        double *a = s_acc + (size_t)fi * sc.acc_stride + (threadIdx.x >> 5) * sc.small_stride;  // this warp's sums
+        double *a_chan = s_acc + (size_t)fi * sc.acc_stride + (blockDim.x >> 5) * sc.small_stride;
         GridRecord<NPOL> rec;
         grid_single_facet<NPOL>(in, vs, js, f, gp, s_n0m1[fi], rec);
-        warp_add_block_sums<NPOL, true>(vs, js, f, gp, b, rec, npol_used, a, a_sumj, a_sumj + 2 * f.nband, jc);
+        warp_add_block_sums<NPOL, true>(vs, js, f, gp, b, rec, npol_used, a, a + f.nband * f.npol, a_chan, jc);
         scatter_any<NPOL, SLOTS>(rec, f, npol_used, lt, ltt, lane, sc.tiles ? wtile : nullptr);
       }
     }
   }
-  if (cur >= 0) flush_grid_sums(sf, npk, s_acc, sc.acc_stride, js, vs.nchan);
+  if (cur >= 0) flush_grid_sums(sf, npk, s_acc, sc, js, vs.nchan);
 }
 
 // Averaged BDA blocks: each warp walks its 32 blocks for every facet of the pack in turn
@@ -161,8 +167,8 @@ __global__ void __launch_bounds__(128, 3) grid_block_q(const ddfg_vis vs, const 
         for (int fi = 0; fi < npk; ++fi) {
           const ddfg_facet &f = sf[fi];
           const int npol_used = min(gp.nvispol, f.npol);
-          double *a = s_acc + (size_t)fi * sc.acc_stride;
-          double *a_chan = a + f.nband * f.npol + 2 * f.nband;
+          double *a = s_acc + (size_t)fi * sc.acc_stride + (threadIdx.x >> 5) * sc.small_stride;
+          double *a_chan = s_acc + (size_t)fi * sc.acc_stride + (blockDim.x >> 5) * sc.small_stride;
           BlockMeans bm{};
           if (lane == 0) bm = grid_block_means(vs, f, bl);
           GridRecord<NPOL> rec;
@@ -185,17 +191,17 @@ __global__ void __launch_bounds__(128, 3) grid_block_q(const ddfg_vis vs, const 
       for (int fi = 0; fi < npk; ++fi) {
         const ddfg_facet &f = sf[fi];
         const int npol_used = min(gp.nvispol, f.npol);
-        double *a = s_acc + (size_t)fi * sc.acc_stride;
+        double *a = s_acc + (size_t)fi * sc.acc_stride + (threadIdx.x >> 5) * sc.small_stride;
+        double *a_chan = s_acc + (size_t)fi * sc.acc_stride + (blockDim.x >> 5) * sc.small_stride;
         GridRecord<NPOL> rec;
         rec.valid = false;
         if (mine) grid_block_record<NPOL>(vs, js, f, gp, b, s_n0m1[fi], rec, jc);
-        warp_add_block_sums<NPOL, false>(vs, js, f, gp, b, rec, npol_used, a, a + f.nband * f.npol,
-                                         a + f.nband * f.npol + 2 * f.nband, jc);
+        warp_add_block_sums<NPOL, false>(vs, js, f, gp, b, rec, npol_used, a, a + f.nband * f.npol, a_chan, jc);
         scatter_any<NPOL, SLOTS>(rec, f, npol_used, lt, ltt, lane, sc.tiles ? wtile : nullptr);
       }
     }
   }
-  if (cur >= 0) flush_grid_sums(sf, npk, s_acc, sc.acc_stride, js, vs.nchan);
+  if (cur >= 0) flush_grid_sums(sf, npk, s_acc, sc, js, vs.nchan);
 }
 
 // grid += grid_lo; grid_lo = 0, for every facet of the table that has a compensation buffer.
@@ -261,7 +267,8 @@ int ddfg_launch_grid(const ddfg_vis *vs, const ddfg_jones *js, const ddfg_facet 
   gp.nvispol = nvispol;
   gp.dopsf = dopsf;
   gp.freq_mean0 = vs->freq_mean;
-  const int acc_stride = max_band + 2 * vs->nchan;
+  const int nwarps_cta = vs->single_vis_blocks ? 8 : 4;
+  const int acc_stride = nwarps_cta * max_band + 2 * vs->nchan;
   const size_t per_facet_smem = sizeof(ddfg_facet) + sizeof(double) + sizeof(double) * (size_t)acc_stride;
   // Shared memory per CTA: two 256-thread CTAs (single-visibility maps) or three 128-thread CTAs
   // (averaged blocks) per SM, each with the warps' grid tiles (one Stokes plane) and the shared
@@ -294,6 +301,7 @@ int ddfg_launch_grid(const ddfg_vis *vs, const ddfg_jones *js, const ddfg_facet 
     sc.npacks = (n + want - 1) / want;
     sc.max_pack = (n + sc.npacks - 1) / sc.npacks;
     sc.acc_stride = acc_stride;
+    sc.small_stride = max_band;
     sc.tiles = tiles;
     sc.nstripes = nstripes;
     // default: items of 16-256 stripes, about four per resident CTA and pack

@@ -24,7 +24,9 @@ struct Sched {
   int nfacets;               // facets of this launch
   int npacks;
   int max_pack;              // most facets in one pack (shared-memory sizing)
-  int acc_stride;            // doubles of one facet's shared accumulators (gridding), 0 otherwise
+  int acc_stride;            // doubles of one facet's shared accumulators (gridding), 0 otherwise:
+                             // [warps][small_stride] weight/Jones sums, then [2][nchan] channel sums
+  int small_stride;          // doubles of one warp's weight and Jones sums of one facet
   int tiles;                 // 1: the warps have grid tiles (scatter_tile) at the start of shared memory
   long long nstripes;        // stripes of 32 blocks
   long long spi;             // stripes per item

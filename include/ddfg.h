@@ -263,6 +263,22 @@ int ddfg_bda_mode1_write(const double *uvw, const int32_t *rows, const int64_t *
                          const int64_t *blk_off, const int64_t *word_off, int32_t *sizes, int32_t *body,
                          void *stream);
 
+/* ---- BDA block maps on the GPU (mode 2) -----------------------------------------------------
+ * Replace GiveBlocksRowsListBL (DDFacet/Data/ClassSmearMapping.py:348-491), per baseline: time
+ * blocks are the runs of equal int32(cumsum(delta_phase) / dphi) with delta_phase the phase change
+ * between consecutive rows at the field edge (2 pi nu0 / 3e8 (|(du, dv)| l_max + |dw| n_max)),
+ * channel blocks of int32(ceil(nchan / ceil(nchan / max(min dnu / dfreq, 1)))) channels cut where
+ * the grid band changes.  Same arguments and two passes as mode 1 (l_max in place of l); the count
+ * pass sets nblk[b] = -1 for a baseline with a single row, which the reference cannot map either
+ * (it reads the second-to-last row difference). */
+int ddfg_bda_mode2_count(const double *uvw, const int32_t *rows, const int64_t *bl_off, int32_t nbl,
+                         int32_t nchan, const int32_t *chan_map, double dfreq, double dphi, double l_max, double nu0,
+                         int64_t *nblk, int64_t *nwords, void *stream);
+int ddfg_bda_mode2_write(const double *uvw, const int32_t *rows, const int64_t *bl_off, int32_t nbl,
+                         int32_t nchan, const int32_t *chan_map, double dfreq, double dphi, double l_max, double nu0,
+                         const int64_t *blk_off, const int64_t *word_off, int32_t *sizes, int32_t *body,
+                         void *stream);
+
 /* Most blocks ddfg_bda_plan_noalloc accepts. */
 #define DDFG_BDA_PLAN_NOALLOC_MAX_BLOCKS (1 << 24)
 

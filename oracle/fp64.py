@@ -175,3 +175,72 @@ def block_indices(uvw, flags, freqs, chan_map, bda_map, wplanes, wconj, overs, r
       int(overs), C.c_double(ref_wave), C.c_double(wmax), int(npix), int(npix), int(nband), C.c_double(incr[0]),
       C.c_double(incr[1]), C.c_double(cu), C.c_double(cv), int(bool(degrid)), _p(out))
     return out[:nb]
+
+
+def predict_np(bda_map, uvw, freqs, chan_map, a0, a1, facets, kms=None, kms_tmap=None, kms_cmap=None,
+               only=None):
+    """Per-facet FP64 predictions P_f (complex128 [nrow][nchan][4]) of the differentiable prediction
+    P = sum_f J0 (s_f I) J1^H exp(+2 pi i nu (u l0 + v m0 + w (n0 - 1)) / c), s_f the degridder's tap
+    sum sum CF G_f at each block's footprint (Stokes I from four linear correlations, XX = YY = I;
+    kMS Jones at the facet's direction per visibility, no normalisation; no smearing), in numpy
+    float64 with complex128 grids and Jones -- so finite differences can take steps float32 cannot
+    hold.  The integer footprints come from block_indices (the FP64 restatement of
+    degridder.h:138-200).  facets: dicts with grid (complex [1][1][N][N]), wplanes, wconj, overs,
+    ref_wave, wmax, incr, cu, cv, l0, m0, idir.  ``only``: indices of the facets to evaluate."""
+    bm = np.ascontiguousarray(bda_map, np.int32)
+    nb = int(np.uint32(bm[0])) + (int(bm[1]) << 32)
+    sizes = bm[2:2 + nb].astype(np.int64)
+    starts = 2 + nb + np.concatenate([[0], np.cumsum(sizes)[:-1]]).astype(np.int64)
+    nrow = uvw.shape[0]
+    nchan = len(freqs)
+    # visibilities of every block: (block, row, channel)
+    vb, vr, vc = [], [], []
+    for b in range(nb):
+        s = starts[b]
+        c0, c1 = int(bm[s]), int(bm[s + 1])
+        rows = bm[s + 2:s + sizes[b]]
+        rr, cc = np.meshgrid(rows, np.arange(c0, c1), indexing="ij")
+        vb.append(np.full(rr.size, b))
+        vr.append(rr.ravel())
+        vc.append(cc.ravel())
+    vb, vr, vc = np.concatenate(vb), np.concatenate(vr).astype(np.int64), np.concatenate(vc).astype(np.int64)
+    flags = np.zeros((nrow, nchan, 4), np.uint8)
+    k_nu = np.asarray(freqs, np.float64) / 299792458.0
+    out = []
+    for fi, f in enumerate(facets):
+        if only is not None and fi not in only:
+            out.append(None)
+            continue
+        G = np.asarray(f["grid"], np.complex128)[0, 0]
+        N = G.shape[-1]
+        idx = block_indices(uvw, flags, freqs, chan_map, bm, f["wplanes"], f["wconj"], f["overs"], f["ref_wave"],
+                            f["wmax"], f["incr"], f["cu"], f["cv"], 1, N, degrid=True)
+        planes = list(f["wconj"]) + list(f["wplanes"])   # the degridder's table order
+        O = int(f["overs"])
+        sblk = np.zeros(nb, np.complex128)
+        ok = idx[:, 0] == 1
+        for p in np.unique(idx[ok, 2]):
+            sel = np.flatnonzero(ok & (idx[:, 2] == p))
+            S = planes[p].shape[0] // O
+            sup = (S - 1) // 2
+            sub = np.asarray(planes[p], np.complex128).reshape(O * O, S, S)[idx[sel, 7]]
+            ry = idx[sel, 4][:, None] - sup + np.arange(S)[None, :]
+            rx = idx[sel, 3][:, None] - sup + np.arange(S)[None, :]
+            win = G[ry[:, :, None], rx[:, None, :]]
+            sblk[sel] = np.sum(sub * win, axis=(1, 2))
+        s = sblk[vb]
+        n0m1 = np.sqrt(1.0 - f["l0"] ** 2 - f["m0"] ** 2) - 1.0
+        u = uvw[vr]
+        ph = np.exp(2j * np.pi * k_nu[vc] * (u[:, 0] * f["l0"] + u[:, 1] * f["m0"] + u[:, 2] * n0m1))
+        P = np.zeros((nrow, nchan, 4), np.complex128)
+        if kms is not None:
+            J = np.asarray(kms, np.complex128)
+            t, ch = np.asarray(kms_tmap)[vr], np.asarray(kms_cmap)[vc]
+            J0 = J[t, f["idir"], np.asarray(a0)[vr], ch].reshape(-1, 2, 2)
+            J1 = J[t, f["idir"], np.asarray(a1)[vr], ch].reshape(-1, 2, 2)
+            M = np.einsum("nij,nkj->nik", J0, np.conj(J1))             # J0 J1^H
+        else:
+            M = np.broadcast_to(np.eye(2, dtype=np.complex128), (vr.size, 2, 2))
+        P[vr, vc, :] = (M.reshape(-1, 4) * (s * ph)[:, None])
+        out.append(P)
+    return out

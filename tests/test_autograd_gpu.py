@@ -1,7 +1,10 @@
 """Differentiable prediction (ddfacet_b200.autograd): the backward kernels against three checks.
 
 * dot-product test: <A x, y> = <x, A^H y> for random model grids x and visibility-space y
-  (32 pairs), relative difference <= 1e-6 in the mean and 1e-5 for any pair;
+  (256 pairs on single-visibility maps, 64 on averaged blocks): norm-wise <= 1e-6 for every pair,
+  relative <= 1e-6 in the mean;
+* central differences with h = 1e-6 in float64 (numpy FP64 prediction on complex128 inputs) at 64
+  coordinates, and the same checks at the benchmark's 81-facet geometry;
 * central finite differences of a float64 loss, L = 1/2 sum w |V - P|^2 with P from the FP64
   oracle degridder, at 64 random coordinates of the model grids and of the kMS Jones array
   (perturbations of 2^-10, exactly representable in the float32 inputs; L is a polynomial, so
@@ -58,23 +61,153 @@ def _vdot(a, b):
     return complex(torch.sum(torch.conj(a.to(torch.complex128)) * b.to(torch.complex128)).item())
 
 
-@pytest.mark.parametrize("kind,jones_mode", [("single", 1), ("bda", 1), ("bda", 2)])
-def test_dot_product_adjoint(kind, jones_mode):
-    cs, setup = _setup(jones=True, kind=kind, jones_mode=jones_mode)
-    rng = np.random.default_rng(0)
+def _dot_product_errors(setup, shape_v, rng, npairs):
+    """|<y, A x> - <A^H y, x>| over npairs random pairs, in float64, relative to |<y, A x>| and
+    norm-wise (relative to ||y|| ||A x||, the Cauchy-Schwarz bound of either product)."""
     kms = setup.jones.kms
-    errs = []
-    for _ in range(32):
+    rel, nw = [], []
+    for _ in range(npairs):
         x = [g.requires_grad_(True) for g in _rand_grids(setup, rng)]
-        y = torch.from_numpy((rng.standard_normal(cs[0].vis.shape) +
-                              1j * rng.standard_normal(cs[0].vis.shape)).astype(np.complex64)).cuda()
+        y = torch.from_numpy((rng.standard_normal(shape_v) + 1j * rng.standard_normal(shape_v))
+                             .astype(np.complex64)).cuda()
         P = predict(setup, x, kms)
         gx = torch.autograd.grad(P, x, grad_outputs=y)
         lhs = _vdot(y, P.detach())
         rhs = sum(_vdot(g, xi.detach()) for g, xi in zip(gx, x))
-        errs.append(abs(lhs - rhs) / abs(lhs))
-    print(f"dot-product test ({kind}, Jones mode {jones_mode}): mean rel {np.mean(errs):.2e}  max {np.max(errs):.2e}")
-    assert np.mean(errs) < 1e-6 and np.max(errs) < 1e-5
+        rel.append(abs(lhs - rhs) / abs(lhs))
+        nw.append(abs(lhs - rhs) / (float(torch.linalg.vector_norm(y.double())) *
+                                    float(torch.linalg.vector_norm(P.detach().to(torch.complex128)))))
+    return np.array(rel), np.array(nw)
+
+
+@pytest.mark.parametrize("kind,jones_mode,npairs", [("single", 1, 256), ("bda", 1, 64), ("bda", 2, 64)])
+def test_dot_product_adjoint(kind, jones_mode, npairs):
+    """Norm-wise <= 1e-6 for every pair.  Relative to the product itself: <= 1e-6 in the mean; the
+    largest is stated -- float32 operators give each product a rounding error of ~eps sqrt(n) times
+    its terms' size, and a pair whose terms cancel (|<y, A x>| well below ||y|| ||A x||) shows it
+    magnified."""
+    cs, setup = _setup(jones=True, kind=kind, jones_mode=jones_mode)
+    rel, nw = _dot_product_errors(setup, cs[0].vis.shape, np.random.default_rng(0), npairs)
+    print(f"dot-product test ({kind}, Jones mode {jones_mode}, {npairs} pairs): norm-wise max {nw.max():.2e}; "
+          f"relative mean {rel.mean():.2e} max {rel.max():.2e}")
+    assert nw.max() < 1e-6
+    assert rel.mean() < 1e-6 and rel.max() < 1e-5
+
+
+def _np_facets(cs, grids):
+    return [dict(grid=g.astype(np.complex128), wplanes=c.wt.Wplanes, wconj=c.wt.WplanesConj, overs=int(c.winfos[3]),
+                 ref_wave=c.wt.RefWave, wmax=c.wt.wmax, incr=c.incr, cu=c.wt.Cu, cv=c.wt.Cv, l0=c.lm[0], m0=c.lm[1],
+                 idir=c.jones["idir_kms"]) for c, g in zip(cs, grids)]
+
+
+def _fd_check(bda, uvw, freqs, chan_map, a0, a1, facets, kms, tmap, cmap, V, w, g_grids, g_kms, rng, ncoord, h=1e-6):
+    """Central differences of L = 1/2 sum w |V - sum_f P_f|^2 at h (float64 steps on complex128
+    grids and Jones) at ncoord random coordinates, half Jones and half model grid, against the GPU
+    gradient: norm-wise relative differences (Jones, grids)."""
+    from oracle import fp64
+
+    kms = np.asarray(kms, np.complex128)
+    Ps = fp64.predict_np(bda, uvw, freqs, chan_map, a0, a1, facets, kms, tmap, cmap)
+    total = sum(Ps)
+    wv = np.asarray(w, np.float64)[:, :, None]
+    Vd = np.asarray(V, np.complex128)
+
+    def dloss(aff, Pp, Pm):
+        """L(+h) - L(-h) without forming L: with r = V - P, |r+|^2 - |r-|^2 = Re[(r+ - r-) conj(r+ + r-)],
+        r+ - r- = -(P+ - P-) and r+ + r- = 2 (V - P_others) - (P+ + P-), so the large |V|^2 terms
+        never meet the small difference."""
+        dp = sum(Pp[i] for i in aff) - sum(Pm[i] for i in aff)
+        sp = 2 * (Vd - (total - sum(Ps[i] for i in aff))) - (sum(Pp[i] for i in aff) + sum(Pm[i] for i in aff))
+        return 0.5 * float(np.sum(wv * np.real(-dp * np.conj(sp))))
+
+    used_t = np.unique(tmap)
+    fd, an = [], []
+    for n in range(ncoord):
+        imag = bool(rng.integers(2))
+        step = 1j * h if imag else h
+        if n < ncoord // 2:  # a Jones coordinate of a direction some facet uses
+            fi = int(rng.integers(len(facets)))
+            d = facets[fi]["idir"]
+            idx = (int(rng.choice(used_t)), d, int(rng.integers(0, kms.shape[2])), 0, int(rng.integers(2)),
+                   int(rng.integers(2)))
+            aff = [i for i, f in enumerate(facets) if f["idir"] == d]
+            Pn = []
+            for sgn in (1, -1):
+                k2 = kms.copy()
+                k2[idx] += sgn * step
+                Pn.append(fp64.predict_np(bda, uvw, freqs, chan_map, a0, a1, facets, k2, tmap, cmap, only=aff))
+            dl = dloss(aff, Pn[0], Pn[1])
+            g = g_kms[idx]
+        else:
+            fi = int(rng.integers(len(facets)))
+            nz = np.argwhere(np.abs(g_grids[fi]) > 0)
+            idx = tuple(nz[rng.integers(len(nz))])
+            Pn = []
+            for sgn in (1, -1):
+                f2 = [dict(f) for f in facets]
+                gg = f2[fi]["grid"].copy()
+                gg[idx] += sgn * step
+                f2[fi]["grid"] = gg
+                Pn.append(fp64.predict_np(bda, uvw, freqs, chan_map, a0, a1, f2, kms, tmap, cmap, only=[fi]))
+            dl = dloss([fi], Pn[0], Pn[1])
+            g = g_grids[fi][idx]
+        fd.append(dl / (2 * h))
+        an.append(g.imag if imag else g.real)
+    fd, an = np.array(fd), np.array(an)
+    k = ncoord // 2
+    return (np.linalg.norm(fd[:k] - an[:k]) / np.linalg.norm(fd[:k]),
+            np.linalg.norm(fd[k:] - an[k:]) / np.linalg.norm(fd[k:]))
+
+
+@pytest.mark.parametrize("kind", ["single", "bda"])
+def test_finite_differences_h1e6(kind):
+    """Central differences with h = 1e-6 in float64 (complex128 grids and Jones through the numpy
+    FP64 prediction, oracle/fp64.py predict_np) at 64 random coordinates -- 32 of the kMS Jones, 32
+    of the model grids -- against the GPU gradient: norm-wise <= 1e-5."""
+    cs, setup = _setup(jones=True, kind=kind, jones_mode=1)
+    rng = np.random.default_rng(11)
+    grids = [g.cpu().numpy() * np.float32(0.01) for g in _rand_grids(setup, rng)]
+    kms = np.ascontiguousarray(cs[0].jones["kms"], np.complex64)
+    V, w = cs[0].vis, cs[0].weights
+    gg, gk, _ = _gpu_loss_grads(setup, grids, kms, V, w)
+    j = cs[0].jones
+    ej, eg = _fd_check(cs[0].bda, cs[0].uvw, cs[0].freqs, cs[0].chan_map, j["A0"], j["A1"], _np_facets(cs, grids), kms,
+                       j["kms_tmap"], j["kms_cmap"], V, w, gg, gk, rng, 64)
+    print(f"central differences h=1e-6 (FP64, {kind}) vs GPU gradient: Jones {ej:.2e}  grid {eg:.2e}")
+    assert ej < 1e-5 and eg < 1e-5
+
+
+def test_config4_geometry():
+    """The differentiation checks at the benchmark's multi-facet geometry (81 facets of 735^2, 32
+    w-planes, 64 channels, 4 correlations) on two dumps, with a 300-source sky and Jones of sigma
+    0.15: dot-product test on 32 pairs (norm-wise <= 1e-6) and central differences (h = 1e-6, FP64)
+    at 16 coordinates (<= 1e-5 norm-wise)."""
+    from ddfacet_b200 import bda, configs
+
+    w = configs.multifacet_dde(device=torch.device("cuda", 0), scale=0.001, nsrc=300, jones_sigma=0.15)
+    setup = PredictSetup(vs=w.vs, facets=w.facets_model, pol=w.pol, jones=w.jones)
+    rng = np.random.default_rng(13)
+    rel, nw = _dot_product_errors(setup, tuple(w.vs.vis.shape), rng, 32)
+    print(f"config-4 geometry ({w.nrow} rows x {w.nchan} ch, 81 facets): dot-product norm-wise max {nw.max():.2e}, "
+          f"relative mean {rel.mean():.2e} max {rel.max():.2e}")
+    assert nw.max() < 1e-6
+    obs = w.host["obs"]
+    grids = [(f.grid * 10).cpu().numpy() for f in w.facets_model]
+    kms = w.jones.kms.cpu().numpy()
+    V = w.vs.vis.cpu().numpy()
+    wt = w.vs.weights.cpu().numpy()
+    x = [torch.from_numpy(g).cuda().requires_grad_(True) for g in grids]
+    k = torch.from_numpy(kms).cuda().requires_grad_(True)
+    r = torch.from_numpy(V).cuda() - predict(setup, x, k)
+    (0.5 * torch.sum(torch.from_numpy(wt).cuda()[:, :, None] * (r.real ** 2 + r.imag ** 2))).backward()
+    facets = [dict(grid=g.astype(np.complex128), wplanes=wtm.Wplanes, wconj=wtm.WplanesConj, overs=11,
+                   ref_wave=wtm.RefWave, wmax=wtm.wmax, incr=fm.incr, cu=wtm.Cu, cv=wtm.Cv, l0=fm.l0, m0=fm.m0,
+                   idir=fm.idir_kms) for g, wtm, fm in zip(grids, w.host["wterms"], w.facets_model)]
+    ej, eg = _fd_check(bda.plain_map(obs.A0, obs.A1, w.nchan), obs.uvw, obs.freqs, w.host["chan_map"], obs.A0, obs.A1,
+                       facets, kms, w.jones.kms_tmap.cpu().numpy(), np.zeros(w.nchan, np.int32), V, wt,
+                       [xi.grad.cpu().numpy() for xi in x], k.grad.cpu().numpy(), rng, 16)
+    print(f"config-4 geometry central differences h=1e-6 vs GPU gradient: Jones {ej:.2e}  grid {eg:.2e}")
+    assert ej < 1e-5 and eg < 1e-5
 
 
 def _oracle_loss(cs, grids, kms, V, w):
