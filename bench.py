@@ -477,6 +477,24 @@ def run_gpu(args):
         e2e_ms = float(t.item())
     del piped
 
+    # The gridder without compensation (plain float32 grid sums), for comparison: one call.
+    plain_grid_ms = None
+    if comp:
+        lo = [f.grid_lo for f in w.facets_grid]
+        for f in w.facets_grid:
+            f.grid_lo = None
+        bnc = D.Batch.create(dev, facets_per_pack=bg.facets_per_pack, stripes_per_item=bg.stripes_per_item)
+        D.grid(w.vs, w.facets_grid, w.pol, w.jones, batch=bnc)
+        torch.cuda.synchronize()
+        u0, u1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        u0.record(stream)
+        D.grid(w.vs, w.facets_grid, w.pol, w.jones, batch=bnc)
+        u1.record(stream)
+        torch.cuda.synchronize()
+        plain_grid_ms = u0.elapsed_time(u1)
+        for f, g in zip(w.facets_grid, lo):
+            f.grid_lo = g
+
     # The plain path on the same chunk: one facet per call.
     plain_step()
     torch.cuda.synchronize()
@@ -524,9 +542,11 @@ def run_gpu(args):
     dom_ms = max(grid_ms, degrid_ms)
     dom_bytes = grid_b if dom == "grid" else degrid_b
     achieved = dom_bytes / (dom_ms * 1e-3) / 1e9
-    # DRAM bytes (read + write) per launch of the dominant kernel, from the ncu capture of the
-    # 0.02-scale chunk (profiles/), per visibility, scaled to this chunk's visibilities
-    traffic_per_vis = {"grid": 192.0, "degrid": 60.0}
+    # DRAM bytes (read + write) of one call of each kernel, per visibility, from the one-pass ncu
+    # capture of the full chunk with the benchmark's schedules (profiles/traffic_combined_at_scale_full.md):
+    # grid 279.4 GB in one launch, degrid 185.1 GB in eight launches of 16 facets (each re-reads and
+    # rewrites the visibilities), for 232,243,200 visibilities
+    traffic_per_vis = {"grid": 279.424e9 / 232243200, "degrid": 185.078e9 / 232243200}
     K, F, G = w.ncorr, w.nfacets, w.info["npix_padded"]
     launches_grid = math.ceil(F / 128) * (2 if comp else 1)
     dpp = bd.facets_per_pack if bd.facets_per_pack > 0 else 128
@@ -571,6 +591,7 @@ def run_gpu(args):
                   "what": "the same kernels, one facet per call (one launch per facet and direction), same chunk",
                   "batched_speedup": round(plain_ms / ms_step, 3)},
         "schedule": dict(tuned.describe(), tune_s=round(t_tune, 1)),
+        "uncompensated_grid_ms": None if plain_grid_ms is None else round(plain_grid_ms, 1),
         "differentiation": diff_info,
         "roofline": {
             "bound": "hbm", "kernel": dom, "achieved": round(achieved, 2), "peak": hbm_peak, "unit": "GB/s",
@@ -579,7 +600,8 @@ def run_gpu(args):
             "alg_bytes_per_launch": int(dom_bytes),
             "how": ("achieved = compulsory bytes of one call (visibilities, flags, weights, uvw, grids, one CF "
                     "table set, Jones; one launch per call) / the call's CUDA-event time; traffic = DRAM "
-                    "read+write per visibility of the ncu capture (0.02-scale chunk) x visibilities"),
+                    "read+write of one call in the one-pass ncu capture of the full chunk, per visibility x "
+                    "visibilities"),
             "fp32": {"achieved_tflops": round(flops_call / (dom_ms * 1e-3) / 1e12, 3),
                      "peak_tflops": round(fp32_peak, 1), "peak_kind": "measured (cuBLAS SGEMM, TF32 off)",
                      "frac": round(flops_call / (dom_ms * 1e-3) / 1e12 / fp32_peak, 4),
@@ -668,6 +690,33 @@ def run_uneven(args):
                       "setup_s": round(setup_s, 1)}), flush=True)
 
 
+def run_profile_call(args):
+    """One grid or one degrid call of the workload with a fixed schedule and nothing else on the GPU
+    before it but the data generation: the launch an ncu capture selects with -k and -c."""
+    import torch
+
+    from ddfacet_b200 import configs, device as D
+
+    dev = torch.device("cuda", 0)
+    w = (configs.multifacet_dde if args.workload == "multifacet_dde" else configs.combined_at_scale)(
+        device=dev, scale=args.scale, keep_host=False)
+    if not args.no_compensation:
+        for f in w.facets_grid:
+            f.with_compensation()
+    b = D.Batch.create(dev, facets_per_pack=args.fpp, stripes_per_item=args.spi, tiles=args.tiles)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    if args.profile_call == "grid":
+        D.grid(w.vs, w.facets_grid, w.pol, w.jones, batch=b)
+    else:
+        D.degrid(w.vs, w.facets_model, w.pol, w.jones, batch=b)
+    e1.record()
+    torch.cuda.synchronize()
+    print(json.dumps({"call": args.profile_call, "ms": round(e0.elapsed_time(e1), 3), "nvis": w.nvis,
+                      "schedule": b.describe(), "compensated": not args.no_compensation}), flush=True)
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -714,9 +763,16 @@ def main():
     ap.add_argument("--retune", action="store_true", help="ignore the autotuner's cache")
     ap.add_argument("--workload", default="combined_at_scale",
                     choices=["combined_at_scale", "multifacet_dde", "uneven_bda"])
+    ap.add_argument("--profile-call", choices=["grid", "degrid"],
+                    help="run one batched call with the schedule below and exit (for ncu captures)")
+    ap.add_argument("--fpp", type=int, default=16, help="--profile-call: facets per pack")
+    ap.add_argument("--spi", type=int, default=64, help="--profile-call: stripes per queue item")
+    ap.add_argument("--tiles", action="store_true", help="--profile-call: warp grid tiles")
 
     args = ap.parse_args()
-    if args.impl == "reference":
+    if args.profile_call:
+        run_profile_call(args)
+    elif args.impl == "reference":
         run_reference(args)
     elif args.workload == "uneven_bda":
         run_uneven(args)
