@@ -5,6 +5,7 @@ NumPy, so the GPU kernels (cuFFT + fused passes) can be compared with it:
   * grid_to_im          -- ClassDDEGridMachine.GridToIm (ClassDDEGridMachine.py:1186-1190) with
                            FFTW_2Donly_np.ifft (ModFFTW.py:631-648);
   * facets_to_im_channel-- ClassFacetMachine.FacetsToIm_Channel (ClassFacetMachine.py:1331-1416);
+  * facet_norm          -- ClassFacetMachine.BuildFacetNormImage (ClassFacetMachine.py:1289-1330);
   * give_model_tessel   -- ClassImToGrid.GiveModelTessel(ToGrid=True) (ClassImToGrid.py:138-264)
                            with FFTW_2Donly_np.fft (ModFFTW.py:611-629);
   * give_model_tessel_adjoint -- the adjoint of give_model_tessel with respect to the real model
@@ -67,7 +68,20 @@ def facets_to_im_channel(dirties, sphes, invsphes, sws_img, weights, pix_central
     return image
 
 
-def give_model_tessel(image, norm_im, sphe, sw_img, xc, yc, n, overs):
+def facet_norm(sws_img, pix_centrals, sizes, npix_out):
+    """BuildFacetNormImage (ClassFacetMachine.py:1289-1330): the sum of the facets' spatial
+    weights (image orientation) placed with GiveEdges, float32."""
+    norm = np.zeros((npix_out, npix_out), np.float32)
+    for sw, (xc, yc), n in zip(sws_img, pix_centrals, sizes):
+        (x0m, x1m, y0m, y1m), (x0f, x1f, y0f, y1f) = give_edges(xc, yc, npix_out, n)
+        norm[x0m:x1m, y0m:y1m] += np.real(np.asarray(sw)[x0f:x1f, y0f:y1f])
+    return norm
+
+
+def give_model_tessel(image, norm_im, sphe, sw_img, xc, yc, n, overs, transform=True):
+    """With ``transform=False`` returns the scaled facet model before the FFT, which is what the
+    reference returns for a facet whose normalised model has no positive pixel (SumFlux == 0,
+    ClassImToGrid.py:249-256)."""
     nch, npol, npix_out, _ = image.shape
     (x0d, x1d, y0d, y1d), (x0p, x1p, y0p, y1p) = give_edges(xc, yc, npix_out, n)
     model = np.zeros((nch, npol, n, n), np.float32)
@@ -80,6 +94,8 @@ def give_model_tessel(image, norm_im, sphe, sw_img, xc, yc, n, overs):
             model[ch, pol][sphe < 1e-3] = 0
             model[ch, pol] = model[ch, pol].T[::-1, :]
     model *= np.float32((overs * n) ** 2)
+    if not transform:
+        return model.astype(np.complex128)
     out = np.zeros(model.shape, np.complex128)
     for ch in range(nch):
         for pol in range(npol):

@@ -21,8 +21,11 @@ The reference's Python modules are imported with stand-ins for the absent option
   maps_golden.npz  ClassJones.GiveTimeMapping / GiveVisToJonesChanMapping and the channel maps
                    ClassVisServer.Init builds (grid bands, channels within bands, degridding bands)
                    for two measurement sets under three frequency settings
+  facets_golden.npz  ClassDDEGridMachine.GridToIm, ClassFacetMachine.BuildFacetNormImage /
+                   FacetsToIm_Channel and ClassImToGrid.GiveModelTessel(ToGrid=True) on a regular
+                   3 x 3 and an uneven 4-facet tessellation of a small image
 
-    python tests/golden/make_golden.py [/path/to/reference] [--only weights|maps]
+    python tests/golden/make_golden.py [/path/to/reference] [--only weights|maps|facets]
 """
 import os
 import sys
@@ -32,7 +35,7 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
-_args = [a for a in sys.argv[1:] if not a.startswith("--") and a not in ("weights", "maps")]
+_args = [a for a in sys.argv[1:] if not a.startswith("--") and a not in ("weights", "maps", "facets")]
 REF = _args[0] if _args else os.environ.get("DDFACET_REF", "")
 if not REF or not os.path.isdir(REF):
     sys.exit("usage: make_golden.py <reference checkout> (or set DDFACET_REF)")
@@ -47,8 +50,14 @@ def _stub(name, **attrs):
 
 
 def _numexpr_evaluate(expr, out=None, casting=None, local_dict=None):
-    """numexpr.evaluate on numpy: evaluates expr with the caller's local variables."""
+    """numexpr.evaluate on numpy: evaluates expr with the caller's local variables, every array
+    operand first cast to their common type (numexpr computes in the widest operand type)."""
     ns = dict(sys._getframe(1).f_locals if local_dict is None else local_dict)
+    names = [k for k in compile(expr, "<numexpr>", "eval").co_names if isinstance(ns.get(k), (np.ndarray, np.generic))]
+    if names:
+        common = np.result_type(*[ns[k].dtype for k in names])
+        for k in names:
+            ns[k] = np.asarray(ns[k]).astype(common, copy=False)
     ns.update(exp=np.exp, sqrt=np.sqrt, sin=np.sin, cos=np.cos, abs=np.abs)
     res = eval(expr, {"__builtins__": {}}, ns)
     if out is not None:
@@ -76,7 +85,7 @@ def import_reference():
     pfi.cache = _stub("pyfftw.interfaces.cache", enable=lambda: None, set_keepalive_time=lambda t: None)
     pfi.scipy_fftpack = _stub("pyfftw.interfaces.scipy_fftpack")
     _stub("SharedArray")
-    _stub("numexpr", evaluate=_numexpr_evaluate)
+    _stub("numexpr", evaluate=_numexpr_evaluate, set_num_threads=lambda n: 1)
     # the process pool imports a compiled helper module at import time; it is never called here
     cb = _stub("DDFacet.cbuild")
     cg = _stub("DDFacet.cbuild.Gridder")
@@ -94,39 +103,48 @@ class CFDict(dict):
         return self[name]
 
 
+class _InertMeta(type):
+    def __getattr__(cls, k):
+        if k.startswith("__"):
+            raise AttributeError(k)
+        return cls
+
+    def __call__(cls, *a, **k):
+        return cls
+
+
+_INERT = _InertMeta("Inert", (), {})
+
+
+class _InertModule(types.ModuleType):
+    """A module every attribute of which is an inert class (imports of names succeed)."""
+    __path__ = []
+
+    def __getattr__(self, k):
+        if k.startswith("__"):
+            raise AttributeError(k)
+        return _INERT
+
+
+def stub(name):
+    """Registers inert modules for ``name`` and its parents that are not importable."""
+    parts = name.split(".")
+    for i in range(1, len(parts) + 1):
+        n = ".".join(parts[:i])
+        if n not in sys.modules:
+            sys.modules[n] = _InertModule(n)
+            if i > 1:
+                setattr(sys.modules[".".join(parts[:i - 1])], parts[i - 1], sys.modules[n])
+
+
 def import_visserver():
     """DDFacet.Data.ClassVisServer with inert stand-ins for the MS, beam and astronomy packages it
     imports at module level (none of them is used by the weight functions), and the compiled
     reference gridder module from oracle/_ref."""
-    class _Meta(type):
-        def __getattr__(cls, k):
-            if k.startswith("__"):
-                raise AttributeError(k)
-            return cls
-
-        def __call__(cls, *a, **k):
-            return cls
-
-    inert = _Meta("Inert", (), {})
-
-    class _Mod(types.ModuleType):
-        __path__ = []
-
-        def __getattr__(self, k):
-            if k.startswith("__"):
-                raise AttributeError(k)
-            return inert
-
-    def stub(name):
-        parts = name.split(".")
-        for i in range(1, len(parts) + 1):
-            n = ".".join(parts[:i])
-            if n not in sys.modules:
-                sys.modules[n] = _Mod(n)
-
     for n in ("pyrap.tables", "pyrap.measures", "pyrap.quanta", "casacore.tables", "casacore.measures",
               "casacore.quanta", "astropy.time", "astropy.io.fits", "astropy.wcs", "ephem"):
-        stub(n)
+        if n not in sys.modules:
+            stub(n)
     sys.path.insert(0, ROOT)
     from oracle import ref
     mod = ref.module()
@@ -279,7 +297,126 @@ def make_maps_golden():
     print("maps golden written")
 
 
+def import_facetmachine():
+    """ClassFacetMachine (FacetsToIm_Channel, BuildFacetNormImage), ClassImToGrid (GiveModelTessel)
+    and ClassDDEGridMachine (GridToIm), with inert stand-ins for the plotting, polygon and image
+    packages and for the compiled modules ClassDDEGridMachine imports at module level (none of
+    them is called by those functions)."""
+    import_visserver()
+    for n in ("pyrap.images", "casacore.images", "matplotlib", "matplotlib.path", "Polygon",
+              "DDFacet.cbuild.Gridder._pyGridderSmearPolsClassic3x", "DDFacet.cbuild.Gridder._pyGridder3x"):
+        stub(n)
+    for _ in range(60):
+        try:
+            from DDFacet.Imager import ClassDDEGridMachine, ClassFacetMachine, ClassImToGrid
+            return ClassFacetMachine, ClassImToGrid, ClassDDEGridMachine
+        except ModuleNotFoundError as e:
+            for k in list(sys.modules):
+                if k.startswith("DDFacet.Imager.Class"):
+                    del sys.modules[k]
+            stub(e.name)
+    raise RuntimeError("could not import ClassFacetMachine")
+
+
+def _cell_sw(ModFFTW, centres, k, xc, yc, n, m, mixing):
+    """Spatial weight of facet k the way _initcf_worker (ClassFacetMachine.py:785-820) makes it,
+    on the facet's padded pixel box [x, y] (image orientation): the facet's tessellation cell
+    (pixels nearer to its centre than to any other centre) inside the main image,
+    Gaussian-smoothed, divided by its maximum, zero below 1e-3."""
+    i, j = np.mgrid[0:n, 0:n]
+    x, y = xc - n // 2 + i, yc - n // 2 + j
+    c = np.asarray(centres, np.float64)
+    d = (x[None] - c[:, 0, None, None]) ** 2 + (y[None] - c[:, 1, None, None]) ** 2
+    mask = (np.argmin(d, axis=0) == k) & (x >= 0) & (x < m) & (y >= 0) & (y < m)
+    sw = np.float32(mask.reshape((1, 1, n, n)))
+    sw = ModFFTW.ConvolveGaussian(shareddict={"in": sw, "out": sw}, field_in="in", field_out="out", ch=0,
+                                  CellSizeRad=1, GaussPars_ch=(mixing, mixing, 0))
+    sw = np.asarray(sw).reshape((n, n))
+    sw /= np.max(sw)
+    sw[sw < 1e-3] = 0.
+    return sw
+
+
+def make_facets_golden():
+    """Stitching and model-image cutting on a regular 3 x 3 and an uneven 4-facet (Voronoi-like)
+    tessellation of a small main image, through the reference's own functions:
+    ClassDDEGridMachine.GridToIm, ClassFacetMachine.BuildFacetNormImage / FacetsToIm_Channel and
+    ClassImToGrid.GiveModelTessel(ToGrid=True)."""
+    ModCF, _, ModFFTW = import_reference()
+    CFM, CIG, CDG = import_facetmachine()
+    rng = np.random.default_rng(77)
+    freqs = np.linspace(1.30e9, 1.45e9, 4)
+    out = {}
+    cases = {
+        # name: main image side, facet centres (pixels), padded facet sizes, bands, Stokes planes
+        "reg": (75, [(12 + 25 * a, 12 + 25 * b) for a in range(3) for b in range(3)], [43] * 9, 2, 1),
+        "vor": (75, [(16, 22), (55, 14), (27, 57), (62, 60)], [61, 57, 67, 49], 1, 2),
+    }
+    for name, (m, centres, sizes, nband, npol) in cases.items():
+        nf = len(centres)
+        fm = types.SimpleNamespace()
+        fm.OutImShape = (nband, npol, m, m)
+        fm.nch, fm.npol, fm.stitchedType = nband, npol, np.float32
+        fm.VS = types.SimpleNamespace(NFreqBands=nband)
+        fm.GD = {"Parallel": {"NCPU": 1}}
+        fm._norm_dict = {}
+        fm.GiveEmptyMainField = lambda _s=fm: np.zeros(_s.OutImShape, dtype=_s.stitchedType)
+        fm.DicoImager, fm._CF, fm.DicoGridMachine = {}, {}, {}
+        for k, ((xc, yc), n) in enumerate(zip(centres, sizes)):
+            cf = CFDict()
+            ModCF.ClassWTermModified(Cell=6.0, Sup=7, Npix=n, Freqs=freqs, wmax=1000.0, Nw=2, OverS=11,
+                                     lmShift=(0.0, 0.0), cf_dict=cf, compute_cf=True)
+            sw = _cell_sw(ModFFTW, centres, k, xc, yc, n, m, 5.0)
+            fm._CF[k] = {"Sphe": np.asarray(cf["Sphe"]), "InvSphe": np.asarray(cf["InvSphe"]), "SW": sw}
+            sumw = rng.uniform(50.0, 200.0, (nband, npol))
+            sjn = rng.uniform(0.5, 2.0, nband)
+            if name == "reg" and k == 0:
+                sumw[1, :] = 0.0  # a band with no weight: stitched without normalisation
+            fm.DicoImager[k] = {"pixCentral": (xc, yc), "NpixFacetPadded": n, "SumWeights": sumw,
+                                "SumJonesNorm": sjn}
+            grid = (rng.standard_normal((nband, npol, n, n)) + 1j * rng.standard_normal((nband, npol, n, n)))
+            grid = grid.astype(np.complex64)
+            gm = types.SimpleNamespace(WTerm=types.SimpleNamespace(OverS=11),
+                                       getFFTWMachine=lambda: ModFFTW.FFTW_2Donly_np())
+            dirty = CDG.ClassDDEGridMachine.GridToIm(gm, grid.copy())
+            fm.DicoGridMachine[k] = {"Dirty": dirty}
+            p = f"{name}_f{k}_"
+            out.update({p + "grid": grid, p + "dirty": np.asarray(dirty, np.complex64), p + "sphe": fm._CF[k]["Sphe"],
+                        p + "invsphe": fm._CF[k]["InvSphe"], p + "sw": sw, p + "sumweights": sumw,
+                        p + "sumjonesnorm": sjn})
+        CFM.ClassFacetMachine.BuildFacetNormImage(fm)
+        norm = np.asarray(fm._norm_dict["FacetNorm"])
+        assert (norm > 0).all(), f"{name}: facet norm has empty pixels"
+        image = CFM.ClassFacetMachine.FacetsToIm_Channel(fm, kind="Dirty")
+        # model image: point components; in the regular case the first facet's padded box holds
+        # negative components only, so the reference's SumFlux is zero there (ClassImToGrid.py:249-256)
+        model = np.zeros((nband, npol, m, m), np.float32)
+        for _ in range(40):
+            x, y = rng.integers(0, m, 2)
+            if name == "reg" and x < 34 and y < 34:
+                continue
+            model[rng.integers(0, nband), rng.integers(0, npol), x, y] = rng.uniform(0.05, 1.0)
+        if name == "reg":
+            model[0, 0, 5, 9], model[1, 0, 14, 3], model[0, 0, 20, 18] = -0.3, -0.2, -0.5
+        i2g = CIG.ClassImToGrid(OverS=11, GD=None)
+        for k in range(nf):
+            g, sumflux = i2g.GiveModelTessel(model, fm.DicoImager, k, norm, fm._CF[k]["Sphe"], fm._CF[k]["SW"],
+                                             ToGrid=True)
+            out[f"{name}_f{k}_model_grid"] = np.asarray(g, np.complex64)
+            out[f"{name}_f{k}_sumflux"] = np.float64(sumflux)
+        out.update({f"{name}_m": m, f"{name}_centres": np.asarray(centres, np.int32),
+                    f"{name}_sizes": np.asarray(sizes, np.int32), f"{name}_nband": nband, f"{name}_npol": npol,
+                    f"{name}_facet_norm": norm, f"{name}_image": np.asarray(image, np.float32),
+                    f"{name}_model": model})
+    out["overs"] = 11
+    np.savez_compressed(os.path.join(HERE, "facets_golden.npz"), **out)
+    print("facets golden written")
+
+
 def main():
+    if ONLY == "facets":
+        make_facets_golden()
+        return
     if ONLY == "weights":
         import_reference()
         make_weights_golden()
