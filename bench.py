@@ -1,7 +1,7 @@
 """Benchmark: Mvis/s through one grid+degrid pass over all facets, on synthetic data.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload combined_at_scale|multifacet_dde|uneven_bda] [--scale S] [--no-compensation]
+                    [--workload combined_at_scale|multifacet_dde|uneven_bda] [--scale S] [--fp32-accumulation]
 
 Default workload: the combined at-scale configuration -- a 10000^2 image at 1 arcsec in 11 x 11
 facets (121 padded grids of 1485^2), 64 antennas, 8 h at 8 s, 256 channels, 4 correlations,
@@ -11,7 +11,7 @@ is one chunk (232.2 M visibilities x 4 correlations, 7.4 GB) through one major-c
 hot path: degrid every facet's model grid and subtract the prediction from the visibilities, then
 grid the residuals onto every facet's residual grid.  Both calls are the batched ones (one
 persistent, queue-driven launch per call, schedule chosen by ddfacet_b200.autotune) with
-compensated (TwoSum) grid sums unless --no-compensation.  ``plain`` in the JSON line times the same
+FP64-accumulated grid sums unless --fp32-accumulation.  ``plain`` in the JSON line times the same
 kernels one facet per call on the same chunk.  The visibilities (7.4 GB) exceed L2, so no flush is
 needed between steps.
 
@@ -168,7 +168,7 @@ def cpu_reference(workload="combined_at_scale", nrow_frac=0.005, nprocs=None):
     return mvis, nprocs, sample
 
 
-def err_vs_fp64(w, compensated, pick=(0, None), sample_rows=None):
+def err_vs_fp64(w, fp64_acc, pick=(0, None), sample_rows=None):
     """Errors of the GPU path against the FP64 restatement (oracle/gridder_fp64.c) on the benchmark's
     own data: the grid of a corner and the centre facet over every row of the chunk (the full
     accumulation depth), and the prediction of the same facets on a row sample."""
@@ -191,18 +191,18 @@ def err_vs_fp64(w, compensated, pick=(0, None), sample_rows=None):
     out = {"grid": {}, "degrid": {}}
     t0 = time.perf_counter()
     fs = [w.facets_grid[i] for i in pick]
-    saved = [(f.grid.clone(), f.grid_lo) for f in fs]
+    saved = [(f.grid.clone(), f.grid_acc) for f in fs]
     for f in fs:
         f.grid.zero_()
-        f.grid_lo = None
-        if compensated:
-            f.with_compensation()
+        f.grid_acc = None
+        if fp64_acc:
+            f.with_fp64_accumulation()
     D.grid(w.vs, fs, w.pol, w.jones, batch=D.Batch.create(dev))
     torch.cuda.synchronize()
     gpu_grids = [f.grid.cpu().numpy() for f in fs]
     for f, (g, lo) in zip(fs, saved):
         f.grid.copy_(g)
-        f.grid_lo = lo
+        f.grid_acc = lo
     for i, g in zip(pick, gpu_grids):
         wt = w.host["wterms"][i]
         fgeo = w.host["tess"].facets[i]
@@ -360,7 +360,7 @@ def run_gpu(args):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     dev = torch.device("cuda", local if world > 1 else 0)
     torch.cuda.set_device(dev)
-    comp = not args.no_compensation
+    comp = not args.fp32_accumulation
 
     t_build = time.perf_counter()
     if args.workload == "multifacet_dde":
@@ -369,7 +369,7 @@ def run_gpu(args):
         w = configs.combined_at_scale(device=dev, scale=args.scale)
     if comp:
         for f in w.facets_grid:
-            f.with_compensation()
+            f.with_fp64_accumulation()
     torch.cuda.synchronize()
     t_build = time.perf_counter() - t_build
     stream = torch.cuda.current_stream()
@@ -477,12 +477,12 @@ def run_gpu(args):
         e2e_ms = float(t.item())
     del piped
 
-    # The gridder without compensation (plain float32 grid sums), for comparison: one call.
+    # The gridder with float32 grid sums (no FP64 accumulator), for comparison: one call.
     plain_grid_ms = None
     if comp:
-        lo = [f.grid_lo for f in w.facets_grid]
+        lo = [f.grid_acc for f in w.facets_grid]
         for f in w.facets_grid:
-            f.grid_lo = None
+            f.grid_acc = None
         bnc = D.Batch.create(dev, facets_per_pack=bg.facets_per_pack, stripes_per_item=bg.stripes_per_item)
         D.grid(w.vs, w.facets_grid, w.pol, w.jones, batch=bnc)
         torch.cuda.synchronize()
@@ -493,7 +493,7 @@ def run_gpu(args):
         torch.cuda.synchronize()
         plain_grid_ms = u0.elapsed_time(u1)
         for f, g in zip(w.facets_grid, lo):
-            f.grid_lo = g
+            f.grid_acc = g
 
     # The plain path on the same chunk: one facet per call.
     plain_step()
@@ -551,16 +551,16 @@ def run_gpu(args):
     launches_grid = math.ceil(F / 128) * (2 if comp else 1)
     dpp = bd.facets_per_pack if bd.facets_per_pack > 0 else 128
     launches_degrid = math.ceil(F / min(dpp, 128))
-    desc = {
-        "combined_at_scale": (f"combined at scale, one 1-h chunk: {F} facets x {G}^2 grids, {w.nrow} rows x "
-                              f"{w.nchan} ch x {K} corr ({nvis/1e6:.1f} Mvis, 7.4 GB) of the 8-h track "
-                              f"({w.info['full_track_nvis']/1e9:.2f} G vis in 8 chunks), per-vis Jones, "
-                              f"{w.info['nw']} w-planes, OverS 11, 1000 point + 20 Gaussian sources; step = degrid "
-                              "all facets (subtract) + grid all facets"),
-        "multifacet_dde": (f"multi-facet DDE: {F} facets x {G}^2 grid, {w.nrow} rows x {w.nchan} ch x {K} corr "
-                           f"({nvis/1e6:.1f} Mvis), per-vis Jones, {w.info['nw']} w-planes, OverS 11; step = degrid "
-                           "all facets (subtract) + grid all facets"),
-    }[args.workload]
+    if args.workload == "combined_at_scale":
+        desc = (f"combined at scale, one 1-h chunk: {F} facets x {G}^2 grids, {w.nrow} rows x "
+                f"{w.nchan} ch x {K} corr ({nvis/1e6:.1f} Mvis, 7.4 GB) of the 8-h track "
+                f"({w.info['full_track_nvis']/1e9:.2f} G vis in 8 chunks), per-vis Jones, "
+                f"{w.info['nw']} w-planes, OverS 11, 1000 point + 20 Gaussian sources; step = degrid "
+                "all facets (subtract) + grid all facets")
+    else:
+        desc = (f"multi-facet DDE: {F} facets x {G}^2 grid, {w.nrow} rows x {w.nchan} ch x {K} corr "
+                f"({nvis/1e6:.1f} Mvis), per-vis Jones, {w.info['nw']} w-planes, OverS 11; step = degrid "
+                "all facets (subtract) + grid all facets")
     out = {
         "metric": METRIC,
         "value": round(value, 3),
@@ -572,7 +572,7 @@ def run_gpu(args):
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
-        "dtype": "f32" + (" (compensated grid sums)" if comp else "") + "; FP64 phase/index arithmetic",
+        "dtype": "f32" + (" (FP64 grid sums)" if comp else "") + "; FP64 phase/index arithmetic",
         "data": "synthetic (seeded; generated on device)",
         "config": {
             "workload": desc, "facets": F, "grid": G, "nvis": nvis, "ncorr": K, "nchan": w.nchan, "nrow": w.nrow,
@@ -583,7 +583,7 @@ def run_gpu(args):
             "l2": f"inputs ({nvis * K * 8 / 1e9:.1f} GB visibilities) larger than L2; no flush",
             "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
             "scale": args.scale,
-            "compensated": comp,
+            "fp64_accumulation": comp,
         },
         "kernels_ms": {"degrid_call": round(degrid_ms, 3), "grid_call": round(grid_ms, 3),
                        "graph_replay_step": round(graph_ms, 3)},
@@ -591,12 +591,12 @@ def run_gpu(args):
                   "what": "the same kernels, one facet per call (one launch per facet and direction), same chunk",
                   "batched_speedup": round(plain_ms / ms_step, 3)},
         "schedule": dict(tuned.describe(), tune_s=round(t_tune, 1)),
-        "uncompensated_grid_ms": None if plain_grid_ms is None else round(plain_grid_ms, 1),
+        "fp32_accumulation_grid_ms": None if plain_grid_ms is None else round(plain_grid_ms, 1),
         "differentiation": diff_info,
         "roofline": {
             "bound": "hbm", "kernel": dom, "achieved": round(achieved, 2), "peak": hbm_peak, "unit": "GB/s",
             "frac": round(achieved / hbm_peak, 6), "peak_kind": peak_kind,
-            "traffic": int(traffic_per_vis[dom] * nvis),
+            "traffic": int(traffic_per_vis[dom] * nvis) if args.workload == "combined_at_scale" else None,
             "alg_bytes_per_launch": int(dom_bytes),
             "how": ("achieved = compulsory bytes of one call (visibilities, flags, weights, uvw, grids, one CF "
                     "table set, Jones; one launch per call) / the call's CUDA-event time; traffic = DRAM "
@@ -644,6 +644,9 @@ def run_uneven(args):
     torch.cuda.synchronize()
     setup_s = time.perf_counter() - t0
     stream = torch.cuda.current_stream()
+    if not args.fp32_accumulation:
+        for f in w.facets_grid:
+            f.with_fp64_accumulation()
     tuned = autotune.tune(w.vs, w.facets_grid, w.facets_model, w.pol, w.jones, use_cache=not args.retune)
 
     def step(batched=True):
@@ -675,10 +678,22 @@ def run_uneven(args):
     step(False)
     torch.cuda.synchronize()
     plain_ms = timed(False, 1)
+
+    def call_ms(fn):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return round(e0.elapsed_time(e1), 1)
+
+    kernels_ms = {"degrid_call": call_ms(lambda: D.degrid(w.vs, w.facets_model, w.pol, w.jones, batch=tuned.degrid)),
+                  "grid_call": call_ms(lambda: D.grid(w.vs, w.facets_grid, w.pol, w.jones, batch=tuned.grid))}
     info = dict(w.info)
     g = info.pop("grids")
     print(json.dumps({"metric": METRIC, "value": round(w.nvis / (ms * 1e-3) / 1e6, 3), "unit": UNIT,
                       "ms_per_step": round(ms, 1), "steps": args.steps, "warmup": max(1, args.warmup),
+                      "kernels_ms": kernels_ms, "fp64_accumulation": not args.fp32_accumulation,
                       "plain": {"ms_per_step": round(plain_ms, 1),
                                 "value": round(w.nvis / (plain_ms * 1e-3) / 1e6, 3),
                                 "batched_speedup": round(plain_ms / ms, 3)},
@@ -700,9 +715,9 @@ def run_profile_call(args):
     dev = torch.device("cuda", 0)
     w = (configs.multifacet_dde if args.workload == "multifacet_dde" else configs.combined_at_scale)(
         device=dev, scale=args.scale, keep_host=False)
-    if not args.no_compensation:
+    if not args.fp32_accumulation:
         for f in w.facets_grid:
-            f.with_compensation()
+            f.with_fp64_accumulation()
     b = D.Batch.create(dev, facets_per_pack=args.fpp, stripes_per_item=args.spi, tiles=args.tiles)
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -714,7 +729,7 @@ def run_profile_call(args):
     e1.record()
     torch.cuda.synchronize()
     print(json.dumps({"call": args.profile_call, "ms": round(e0.elapsed_time(e1), 3), "nvis": w.nvis,
-                      "schedule": b.describe(), "compensated": not args.no_compensation}), flush=True)
+                      "schedule": b.describe(), "fp64_accumulation": not args.fp32_accumulation}), flush=True)
 
 
 def run_reference(args):
@@ -758,7 +773,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--scale", type=float, default=1.0)
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
-    ap.add_argument("--no-compensation", action="store_true", help="plain float32 grid sums")
+    ap.add_argument("--fp32-accumulation", action="store_true", help="float32 grid sums (no FP64 accumulator)")
     ap.add_argument("--no-diff", action="store_true", help="skip the differentiation timing")
     ap.add_argument("--retune", action="store_true", help="ignore the autotuner's cache")
     ap.add_argument("--workload", default="combined_at_scale",

@@ -41,7 +41,7 @@ class Facet(C.Structure):
         ("idir_kms", _i32), ("idir_beam", _i32),
         ("decorr_l", _f64), ("decorr_m", _f64),
         ("sumwt", _vp), ("sumjones", _vp), ("sumjones_chan", _vp),
-        ("grid_lo", _vp),
+        ("grid_acc", _vp),
     ]
 
 

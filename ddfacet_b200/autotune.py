@@ -24,7 +24,7 @@ import torch
 from . import device as D
 
 GRID_CANDIDATES: List[dict] = [dict(facets_per_pack=p, stripes_per_item=s, tiles=t)
-                               for p in (8, 16, 32) for s in (0, 64) for t in (False, True)]
+                               for p in (4, 8, 16, 32) for s in (0, 64) for t in (False, True)]
 DEGRID_CANDIDATES: List[dict] = [dict(facets_per_pack=p, stripes_per_item=s) for p in (16, 32, 0) for s in (0, 64)]
 
 
@@ -36,23 +36,45 @@ def _cache_path() -> str:
 def workload_key(vs: D.VisData, facets: Sequence[D.FacetGrid], pol, jones: Optional[D.JonesData]) -> str:
     """Hash of what the best schedule depends on: grid sizes, facet count, block count (rounded to a
     power of two), channels, correlations, Stokes planes, single-visibility map, supports, Jones mode,
-    compensation, large-block list and the GPU."""
+    FP64 accumulation, large-block list and the GPU."""
     sizes = sorted({tuple(f.grid.shape) for f in facets})
     nb = max(1, int(vs.nblocks))
     desc = dict(sizes=sizes, nfacets=len(facets), nblocks_log2=nb.bit_length(), nchan=int(vs.vis.shape[1]),
                 ncorr=int(vs.vis.shape[2]), npol=int(pol.npol), single=int(vs.single_vis_blocks),
                 sup=max(int(f.cf.max_support) for f in facets), jones=0 if jones is None else int(jones.mode),
-                comp=any(f.grid_lo is not None for f in facets), large=vs.large_blocks is not None,
+                acc64=any(f.grid_acc is not None for f in facets), large=vs.large_blocks is not None,
                 gpu=torch.cuda.get_device_name(vs.vis.device))
     return hashlib.sha1(json.dumps(desc, sort_keys=True, default=str).encode()).hexdigest()[:16]
 
 
 def sample_blocks(vs: D.VisData, nblocks: int) -> D.VisData:
-    """The first ``nblocks`` blocks of ``vs`` (block starts and sparsification cut; the large-block
-    list is kept, the kernels skip its entries beyond the sample)."""
-    n = min(int(nblocks), vs.nblocks)
-    sp = None if vs.sparsification is None else vs.sparsification[:n]
-    return dataclasses.replace(vs, block_start=vs.block_start[:n], nblocks=n, sparsification=sp)
+    """About ``nblocks`` blocks of ``vs`` in whole stripes (32 consecutive blocks, the kernels' unit
+    of work) taken at an even stride over the map, so the sample covers the whole uv coverage of
+    the chunk (and touches the grids the way the full call does) rather than its first rows: a
+    new packed map of those blocks, planned, with its own large-block list when ``vs`` has one."""
+    nb = int(vs.nblocks)
+    nstripes = (nb + 31) // 32
+    want = max(1, min(nstripes, (int(nblocks) + 31) // 32))
+    if want >= nstripes:
+        return vs
+    dev = vs.bda_map.device
+    stripes = torch.div(torch.arange(want, device=dev, dtype=torch.int64) * nstripes, want, rounding_mode="floor")
+    order = (stripes[:, None] * 32 + torch.arange(32, device=dev, dtype=torch.int64)[None, :]).reshape(-1)
+    order = order[order < nb]
+    sizes = vs.bda_map[2:2 + nb].to(torch.int64)[order]
+    starts = vs.block_start[order]
+    total = int(sizes.sum().item())
+    n = int(order.numel())
+    idx = torch.repeat_interleave(starts - (torch.cumsum(sizes, 0) - sizes), sizes) + torch.arange(total, device=dev)
+    m = torch.empty(2 + n + total, dtype=torch.int32, device=dev)
+    m[0], m[1] = n & 0xFFFFFFFF, n >> 32
+    m[2:2 + n] = sizes.to(torch.int32)
+    m[2 + n:] = vs.bda_map[idx]
+    block_start, single = D.VisData.plan_map(m, int(vs.vis.shape[0]), int(vs.vis.shape[1]))
+    sp = None if vs.sparsification is None else vs.sparsification[order].contiguous()
+    out = dataclasses.replace(vs, bda_map=m, block_start=block_start, nblocks=n, single_vis_blocks=single,
+                              sparsification=sp, large_blocks=None, large_min_vis=0)
+    return out.with_large_blocks(vs.large_min_vis) if vs.large_blocks is not None else out
 
 
 def _time(fn, reps: int = 2) -> float:
@@ -107,7 +129,7 @@ def tune(vs: D.VisData, facets_grid: Sequence[D.FacetGrid], facets_model: Sequen
     n = max(min_blocks, int(vs.nblocks * sample_fraction))
     sv = sample_blocks(vs, n)
     scratch = [dataclasses.replace(f, grid=torch.zeros_like(f.grid),
-                                   grid_lo=None if f.grid_lo is None else torch.zeros_like(f.grid_lo),
+                                   grid_acc=None if f.grid_acc is None else torch.zeros_like(f.grid_acc),
                                    sumwt=None if f.sumwt is None else torch.zeros_like(f.sumwt),
                                    sumjones=None if f.sumjones is None else torch.zeros_like(f.sumjones),
                                    sumjones_chan=None if f.sumjones_chan is None else torch.zeros_like(f.sumjones_chan))

@@ -152,6 +152,9 @@ int check_common(const char *who, const ddfg_vis *vs, const ddfg_jones *js, cons
     if (f.nx <= 0 || f.ny <= 0 || f.nband <= 0 || f.npol <= 0 || f.nw <= 0 || f.overs <= 0)
       return ddfg_set_error(DDFG_EINVAL, "%s: facet %d has a bad shape", who, i);
     if (f.wmax == 0.) return ddfg_set_error(DDFG_EINVAL, "%s: facet %d has wmax = 0", who, i);
+    if (((uintptr_t)f.grid & 7) || ((uintptr_t)f.grid_acc & 15))
+      return ddfg_set_error(DDFG_EINVAL, "%s: facet %d grid (8 bytes) or FP64 accumulator (16 bytes) misaligned",
+                            who, i);
     if (f.max_support <= 0 || f.max_support > 63)
       return ddfg_set_error(DDFG_EINVAL, "%s: facet %d max_support %d outside [1, 63]", who, i, f.max_support);
   }

@@ -50,7 +50,7 @@ __global__ void __launch_bounds__(256, SLOTS == 2 ? 2 : 1)
     const long long item = queue_next(sc, &q, static_next);
     if (item >= sc.nitems) break;
     const int pack = (int)(item / sc.items_per_pack);
-    const long long s0 = (item - (long long)pack * sc.items_per_pack - sc.large_items) * sc.spi;
+    const long long s0 = slot_stripe(sc, item - (long long)pack * sc.items_per_pack - sc.large_items);
     if (pack != cur) {
       npk = stage_pack(tab, sc, pack, sf, s_n0m1);
       cur = pack;
@@ -152,7 +152,7 @@ __global__ void __launch_bounds__(256) degrid_block_q(const ddfg_vis vs, const d
       }
       continue;
     }
-    const long long s0 = (r - sc.large_items) * sc.spi;
+    const long long s0 = slot_stripe(sc, r - sc.large_items);
     const int ns = (int)min(sc.spi, sc.nstripes - s0);
     for (int k; (k = warp_take(&q, ns, lane)) >= 0;) {
       const int64_t b = (s0 + k) * 32 + lane;
@@ -183,7 +183,7 @@ namespace {
 
 template <int NP, int SL>
 int launch_degrid_table(const ddfg_vis *vs, const ddfg_jones *js, const FacetTable &tab, const DegridParams &dp,
-                        const Sched &sc, const ddfg_batch *batch, cudaStream_t stream) {
+                        Sched sc, const ddfg_batch *batch, cudaStream_t stream) {
   const bool single = vs->single_vis_blocks != 0;
   const size_t smem = (NP == 1 ? 8 * kPartialBytesPerWarp : 0) + (sizeof(ddfg_facet) + sizeof(double)) * sc.max_pack;
   const void *kern = single ? (const void *)degrid_single_q<NP, SL> : (const void *)degrid_block_q<NP, SL>;
@@ -192,6 +192,7 @@ int launch_degrid_table(const ddfg_vis *vs, const ddfg_jones *js, const FacetTab
   if (rc) return rc;
   if (batch && batch->ctas_per_sm > 0) per_sm = min(per_sm, (int)batch->ctas_per_sm);
   const int ctas = ddfg_num_ctas(per_sm);
+  sched_set_regions(sc, (batch && (batch->flags & 4)) ? ctas : 1);
   if (single) degrid_single_q<NP, SL><<<ctas, 256, smem, stream>>>(*vs, *js, tab, dp, sc);
   else degrid_block_q<NP, SL><<<ctas, 256, smem, stream>>>(*vs, *js, tab, dp, sc);
   const cudaError_t e = cudaGetLastError();
@@ -242,8 +243,7 @@ int ddfg_launch_degrid(const ddfg_vis *vs, const ddfg_jones *js, const ddfg_face
     sc.stripe_items = (nstripes + sc.spi - 1) / sc.spi;
     sc.large_per_item = 8;
     sc.large_items = (nlarge + sc.large_per_item - 1) / sc.large_per_item;
-    sc.items_per_pack = sc.large_items + sc.stripe_items;
-    sc.nitems = sc.items_per_pack * sc.npacks;
+    sched_set_regions(sc, 1);
     sc.counter = counters ? counters + g : nullptr;
     int rc;
 #define LD(NP, SL) rc = launch_degrid_table<NP, SL>(vs, js, tab, dp, sc, batch, stream)

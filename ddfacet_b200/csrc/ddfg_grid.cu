@@ -12,8 +12,8 @@
 //    facet-independent inputs come from DRAM once per pack, the facet-dependent record (position,
 //    Jones, phasor, Stokes) is formed per facet, and the 32 lanes lay each record's S x S taps
 //    (hot loop 2, gridder.h:353-375) onto the facet grid with vector atomics (scatter_q: runs of
-//    records on the same cells merged in registers; TwoSum-compensated when the facet has a
-//    grid_lo buffer);
+//    records on the same cells merged in registers; into an FP64 accumulator when the facet
+//    has a grid_acc buffer, folded into the float32 grid at the end of the call);
 //  * per-band weight sums and the Jones normalisation sums are reduced per warp into shared
 //    accumulators of the pack's facets and flushed when the CTA moves to another pack.
 //
@@ -103,7 +103,7 @@ __global__ void __launch_bounds__(256) grid_single_q(const ddfg_vis vs, const dd
     const long long item = queue_next(sc, &q, static_next);
     if (item >= sc.nitems) break;
     const int pack = (int)(item / sc.items_per_pack);
-    const long long s0 = (item - (long long)pack * sc.items_per_pack - sc.large_items) * sc.spi;
+    const long long s0 = slot_stripe(sc, item - (long long)pack * sc.items_per_pack - sc.large_items);
     enter_pack(tab, sc, js, vs.nchan, pack, cur, npk, sf, s_n0m1, s_acc);
     const int ns = (int)min(sc.spi, sc.nstripes - s0);
     for (int k; (k = warp_take(&q, ns, lane)) >= 0;) {
@@ -138,16 +138,14 @@ __global__ void __launch_bounds__(128, 3) grid_block_q(const ddfg_vis vs, const 
                                                        const __grid_constant__ FacetTable tab, const GridParams gp,
                                                        const Sched sc) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  float2 *wtile = (float2 *)smem_raw + (threadIdx.x >> 5) * kTileCells;  // [warps][kTileCells] if sc.tiles
-  ddfg_facet *sf = (ddfg_facet *)(smem_raw + (sc.tiles ? (blockDim.x >> 5) * kTileCells * sizeof(float2) : 0));
+  ddfg_facet *sf = (ddfg_facet *)smem_raw;
   double *s_n0m1 = (double *)(sf + sc.max_pack);
   double *s_acc = s_n0m1 + sc.max_pack;
   __shared__ QueueSmem q;
   const int lane = threadIdx.x & 31;
   JonesCache jc;
-  LaneTaps<SLOTS> lt, ltt;
+  LaneTaps<SLOTS> lt;
   lt.reset();
-  ltt.reset();
   long long static_next = blockIdx.x;
   int cur = -1, npk = 0;
   for (;;) {
@@ -177,12 +175,12 @@ __global__ void __launch_bounds__(128, 3) grid_block_q(const ddfg_vis vs, const 
           grid_block_record_warp<NPOL>(vs, js, f, gp, bl, bm, s_n0m1[fi], 0, lane, npol_used, a_chan, rec);
           warp_add_block_sums<NPOL, false>(vs, js, f, gp, bl, rec, npol_used, a, a + f.nband * f.npol, a_chan, jc,
                                            !rec.single_chan);
-          scatter_any<NPOL, SLOTS>(rec, f, npol_used, lt, ltt, lane, sc.tiles ? wtile : nullptr);
+          scatter_q<NPOL, SLOTS, false>(rec, f, npol_used, lt, lane);
         }
       }
       continue;
     }
-    const long long s0 = (r - sc.large_items) * sc.spi;
+    const long long s0 = slot_stripe(sc, r - sc.large_items);
     const int ns = (int)min(sc.spi, sc.nstripes - s0);
     for (int k; (k = warp_take(&q, ns, lane)) >= 0;) {
       const int64_t b = (s0 + k) * 32 + lane;
@@ -197,28 +195,28 @@ __global__ void __launch_bounds__(128, 3) grid_block_q(const ddfg_vis vs, const 
         rec.valid = false;
         if (mine) grid_block_record<NPOL>(vs, js, f, gp, b, s_n0m1[fi], rec, jc);
         warp_add_block_sums<NPOL, false>(vs, js, f, gp, b, rec, npol_used, a, a + f.nband * f.npol, a_chan, jc);
-        scatter_any<NPOL, SLOTS>(rec, f, npol_used, lt, ltt, lane, sc.tiles ? wtile : nullptr);
+        scatter_q<NPOL, SLOTS, false>(rec, f, npol_used, lt, lane);
       }
     }
   }
   if (cur >= 0) flush_grid_sums(sf, npk, s_acc, sc, js, vs.nchan);
 }
 
-// grid += grid_lo; grid_lo = 0, for every facet of the table that has a compensation buffer.
-__global__ void fold_lo_kernel(const __grid_constant__ FacetTable tab, int nfacets) {
+// grid = fl(grid + acc); acc = 0, for every facet of the table that has an FP64 accumulator.
+__global__ void fold_acc_kernel(const __grid_constant__ FacetTable tab, int nfacets) {
   const int fi = blockIdx.y;
   if (fi >= nfacets) return;
   const ddfg_facet &f = tab.f[fi];
-  if (!f.grid_lo) return;
-  float2 *hi = (float2 *)f.grid;
-  float2 *lo = (float2 *)f.grid_lo;
+  if (!f.grid_acc) return;
+  float2 *grid = (float2 *)f.grid;
+  double2 *acc = (double2 *)f.grid_acc;
   const int64_t n = (int64_t)f.nband * f.npol * f.ny * f.nx;
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-    const float2 l = lo[i];
-    if (l.x != 0.f || l.y != 0.f) {
-      const float2 h = hi[i];
-      hi[i] = make_float2(h.x + l.x, h.y + l.y);
-      lo[i] = czero();
+    const double2 a = acc[i];
+    if (a.x != 0. || a.y != 0.) {
+      const float2 g = grid[i];
+      grid[i] = make_float2((float)((double)g.x + a.x), (float)((double)g.y + a.y));
+      acc[i] = make_double2(0., 0.);
     }
   }
 }
@@ -243,6 +241,7 @@ int launch_grid_table(const ddfg_vis *vs, const ddfg_jones *js, const FacetTable
   if (rc) return rc;
   if (batch && batch->ctas_per_sm > 0) per_sm = min(per_sm, (int)batch->ctas_per_sm);
   const int ctas = ddfg_num_ctas(per_sm);
+  sched_set_regions(sc, (batch && (batch->flags & 4)) ? ctas : 1);
   if (single) grid_single_q<NP, SL><<<ctas, threads, smem, stream>>>(*vs, *js, tab, gp, sc);
   else grid_block_q<NP, SL><<<ctas, threads, smem, stream>>>(*vs, *js, tab, gp, sc);
   const cudaError_t e = cudaGetLastError();
@@ -255,11 +254,11 @@ int launch_grid_table(const ddfg_vis *vs, const ddfg_jones *js, const FacetTable
 int ddfg_launch_grid(const ddfg_vis *vs, const ddfg_jones *js, const ddfg_facet *facets, int nfacets, int policy,
                      int nvispol, int dopsf, const ddfg_batch *batch, cudaStream_t stream) {
   int max_support = 1, max_band = 1;
-  bool any_lo = false;
+  bool any_acc = false;
   for (int i = 0; i < nfacets; ++i) {
     max_support = max(max_support, facets[i].max_support);
     max_band = max(max_band, facets[i].nband * (facets[i].npol + 2));
-    any_lo = any_lo || facets[i].grid_lo != nullptr;
+    any_acc = any_acc || facets[i].grid_acc != nullptr;
   }
   const int slots = tap_slots(max_support);
   GridParams gp;
@@ -276,7 +275,8 @@ int ddfg_launch_grid(const ddfg_vis *vs, const ddfg_jones *js, const ddfg_facet 
   const bool single = vs->single_vis_blocks != 0;
   const size_t budget = single ? 110 * 1024 : 74 * 1024;
   const size_t tile_bytes = (size_t)(single ? 8 : 4) * kTileCells * sizeof(float2);
-  int tiles = (nvispol == 1 && batch && (batch->flags & 2)) ? 1 : 0;
+  // warp tiles: single-visibility maps (a stripe is one row's neighbouring channels) only
+  int tiles = (single && nvispol == 1 && batch && (batch->flags & 2)) ? 1 : 0;
   if (tiles && budget < tile_bytes + per_facet_smem) tiles = 0;
   const int max_fit = (int)((budget - (tiles ? tile_bytes : 0)) / per_facet_smem);
   if (max_fit < 1) return ddfg_set_error(DDFG_ESIZE, "grid: too many bands/channels for the shared accumulators");
@@ -311,8 +311,7 @@ int ddfg_launch_grid(const ddfg_vis *vs, const ddfg_jones *js, const ddfg_facet 
     sc.stripe_items = (nstripes + sc.spi - 1) / sc.spi;
     sc.large_per_item = vs->single_vis_blocks ? 8 : 4;
     sc.large_items = (nlarge + sc.large_per_item - 1) / sc.large_per_item;
-    sc.items_per_pack = sc.large_items + sc.stripe_items;
-    sc.nitems = sc.items_per_pack * sc.npacks;
+    sched_set_regions(sc, 1);
     sc.counter = counters ? counters + g : nullptr;
     int rc;
 #define LG(NP, SL) rc = launch_grid_table<NP, SL>(vs, js, tab_tl, gp, sc, batch, stream)
@@ -327,7 +326,7 @@ int ddfg_launch_grid(const ddfg_vis *vs, const ddfg_jones *js, const ddfg_facet 
 #undef LG_NP
 #undef LG
     if (rc) return rc;
-    if (any_lo) {
+    if (any_acc) {
       int64_t cells = 0;
       for (int i = 0; i < n; ++i)
         {
@@ -335,7 +334,7 @@ int ddfg_launch_grid(const ddfg_vis *vs, const ddfg_jones *js, const ddfg_facet 
           if (c > cells) cells = c;
         }
       const int bx = (int)((cells + 255) / 256 < 1024 ? (cells + 255) / 256 : 1024);
-      fold_lo_kernel<<<dim3(bx, n), 256, 0, stream>>>(tab_tl, n);
+      fold_acc_kernel<<<dim3(bx, n), 256, 0, stream>>>(tab_tl, n);
       const cudaError_t e = cudaGetLastError();
       if (e != cudaSuccess) return ddfg_set_error(DDFG_ECUDA, "grid fold: %s", cudaGetErrorString(e));
     }

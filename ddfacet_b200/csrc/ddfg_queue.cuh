@@ -1,5 +1,5 @@
 // Persistent, queue-driven scheduling of the gridding and degridding kernels, and the tap
-// scatter they share (run merging, optional compensated accumulation).
+// scatter they share (run merging, optional FP64 accumulation).
 //
 // One launch takes up to DDFG_TABLE_FACETS facet descriptors as a __grid_constant__ parameter
 // table.  The facets are split into packs of balanced size; a work item is a run of stripes
@@ -33,10 +33,32 @@ struct Sched {
   long long stripe_items;    // ceil(nstripes / spi)
   int large_per_item;        // large blocks per item
   long long large_items;     // ceil(nlarge / large_per_item)
-  long long items_per_pack;  // large_items + stripe_items
+  long long regions;         // stripe items interleaved over this many regions (1: in order)
+  long long per_region;      // ceil(stripe_items / regions)
+  long long items_per_pack;  // large_items + stripe item slots (regions * per_region)
   long long nitems;          // npacks * items_per_pack
   unsigned long long *counter;  // item counter (zeroed before the launch), or NULL: static order
 };
+
+// Host: spreads a pack's stripe items over `regions` contiguous regions of the block order, taken
+// in turn, so that CTAs holding consecutive item numbers work far apart in the map (for a map in
+// uv-cell order: far apart on the grids, which keeps concurrent grid additions off the same
+// cells).  With the static order and as many regions as CTAs, each CTA walks one region.
+inline void sched_set_regions(Sched &sc, long long regions) {
+  regions = regions < 1 ? 1 : (regions > sc.stripe_items ? sc.stripe_items : regions);
+  if (regions < 1) regions = 1;
+  sc.regions = regions;
+  sc.per_region = (sc.stripe_items + regions - 1) / regions;
+  sc.items_per_pack = sc.large_items + (regions > 1 ? regions * sc.per_region : sc.stripe_items);
+  sc.nitems = sc.items_per_pack * sc.npacks;
+}
+
+// First stripe of stripe-item slot rr of a pack (0 <= rr < items_per_pack - large_items); slots
+// past the last stripe give a start >= nstripes (an empty item).
+__device__ __forceinline__ long long slot_stripe(const Sched &sc, long long rr) {
+  const long long it = sc.regions > 1 ? (rr % sc.regions) * sc.per_region + rr / sc.regions : rr;
+  return it * sc.spi;
+}
 
 __device__ __forceinline__ int pack_first(const Sched &sc, int p) {
   return (int)(((long long)p * sc.nfacets) / sc.npacks);
@@ -88,31 +110,23 @@ __device__ __forceinline__ int stage_pack(const FacetTable &tab, const Sched &sc
 // Grid additions
 // ----------------------------------------------------------------------------------------
 
-// hi[cell] += v with the rounding error of the addition added to lo[cell] (lo = hi + lo_off):
-// the atomic returns the old value a, the cell now holds fl(a + v), and TwoSum(a, v) recovers
-// fl(a + v) - (a + v) exactly (Knuth, TAOCP vol. 2, 4.2.2).  Summed over a call, hi + lo is the
-// exact sum of the addends up to the (second-order) rounding of lo's own additions.
-// fl(a + v) - (a + v), componentwise, exactly (TwoSum).
-__device__ __forceinline__ float2 two_sum_err(float2 a, float2 v) {
-  const float sx = __fadd_rn(a.x, v.x), sy = __fadd_rn(a.y, v.y);
-  const float bx = __fsub_rn(sx, a.x), by = __fsub_rn(sy, a.y);
-  return make_float2(__fadd_rn(__fsub_rn(a.x, __fsub_rn(sx, bx)), __fsub_rn(v.x, bx)),
-                     __fadd_rn(__fsub_rn(a.y, __fsub_rn(sy, by)), __fsub_rn(v.y, by)));
+// Adds v to a grid cell: into the facet's FP64 accumulator when it has one (two non-returning
+// FP64 atomics; the float32 grid is untouched until the fold), else into the float32 cell.  The
+// accumulator cell of grid cell c is found without the cell's index: with acc_off =
+// addr(acc) - 2 addr(grid), addr(acc[c]) = 2 addr(grid[c]) + acc_off (16-byte cells for 8-byte
+// ones; addresses are below 2^48, so the doubling cannot overflow).
+__device__ __forceinline__ void grid_add(float2 *cell, bool acc, ptrdiff_t acc_off, float2 v) {
+  if (acc) {
+    double *d = (double *)(2 * (intptr_t)cell + acc_off);
+    asm volatile("red.global.add.f64 [%0], %1;" ::"l"(d), "d"((double)v.x) : "memory");
+    asm volatile("red.global.add.f64 [%0], %1;" ::"l"(d + 1), "d"((double)v.y) : "memory");
+  } else {
+    red_add(cell, v);
+  }
 }
 
-__device__ __forceinline__ void comp_add(float2 *cell, ptrdiff_t lo_off, float2 v) {
-  float2 a;
-  asm volatile("atom.global.v2.f32.add {%0, %1}, [%2], {%3, %4};"
-               : "=f"(a.x), "=f"(a.y)
-               : "l"(cell), "f"(v.x), "f"(v.y)
-               : "memory");
-  const float2 e = two_sum_err(a, v);
-  if (e.x != 0.f || e.y != 0.f) red_add(cell + lo_off, e);
-}
-
-__device__ __forceinline__ void grid_add(float2 *cell, bool comp, ptrdiff_t lo_off, float2 v) {
-  if (comp) comp_add(cell, lo_off, v);
-  else red_add(cell, v);
+__device__ __forceinline__ ptrdiff_t acc_offset(const ddfg_facet &f) {
+  return f.grid_acc ? (ptrdiff_t)((intptr_t)f.grid_acc - 2 * (intptr_t)f.grid) : 0;
 }
 
 // Warp-cooperative tap scatter of the warp's 32 records onto facet f (gridder.h:353-362).
@@ -120,14 +134,16 @@ __device__ __forceinline__ void grid_add(float2 *cell, bool comp, ptrdiff_t lo_o
 //  * run merging: consecutive records (lane order) with the same footprint origin and support
 //    add their products into the lane's registers and reach the grid as one addition per tap
 //    (consecutive channels of a row often fall on the same cell); the comparison is warp-uniform;
-//  * compensated additions when the facet has a grid_lo buffer (comp_add).
+//  * FP64 accumulation when the facet has a grid_acc buffer (grid_add).
+// MERGE = false drops the run merging (its accumulators cost registers that the averaged-block
+// kernels, whose stripes rarely repeat a footprint, cannot spare).
 // Must be called by all 32 lanes.
-template <int NPOL, int SLOTS>
+template <int NPOL, int SLOTS, bool MERGE = true>
 __device__ __forceinline__ void scatter_q(const GridRecord<NPOL> &rec, const ddfg_facet &f, int npol_used,
                                           LaneTaps<SLOTS> &lt, int lane) {
   float2 *grid = (float2 *)f.grid;
-  const bool comp = f.grid_lo != nullptr;
-  const ptrdiff_t lo_off = comp ? (float2 *)f.grid_lo - grid : 0;
+  const bool comp = f.grid_acc != nullptr;
+  const ptrdiff_t lo_off = acc_offset(f);
   const float2 *cfd = (const float2 *)f.cf_data;
   const int plane_sz = f.nx * f.ny;
   TapJob job;
@@ -146,6 +162,52 @@ __device__ __forceinline__ void scatter_q(const GridRecord<NPOL> &rec, const ddf
     for (int k = 0; k < SLOTS; ++k) {
       on[k] = lt.off[k] >= 0;
       g_lane[k] = grid + (on[k] ? lt.off[k] : 0);
+    }
+    if constexpr (!MERGE) {
+      while (mask) {
+        int src[4];
+        int nr = 0;
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+          src[r] = mask ? __ffs(mask) - 1 : src[0];
+          if (mask) {
+            mask &= mask - 1;
+            ++nr;
+          }
+        }
+        int base[4], cfo[4];
+        float2 sv[4][NPOL];
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+          base[r] = __shfl_sync(0xffffffffu, job.base, src[r]);
+          cfo[r] = __shfl_sync(0xffffffffu, job.cfoff, src[r]);
+#pragma unroll
+          for (int p = 0; p < NPOL; ++p) {
+            sv[r][p].x = __shfl_sync(0xffffffffu, rec.stokes[p].x, src[r]);
+            sv[r][p].y = __shfl_sync(0xffffffffu, rec.stokes[p].y, src[r]);
+          }
+        }
+        float2 c[4][SLOTS];
+#pragma unroll
+        for (int r = 0; r < 4; ++r)
+#pragma unroll
+          for (int k = 0; k < SLOTS; ++k) c[r][k] = on[k] ? __ldg(cf_lane + cfo[r] + 32 * k) : czero();
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+          if (r < nr) {
+#pragma unroll
+            for (int k = 0; k < SLOTS; ++k) {
+              if (on[k]) {
+                float2 *cell = g_lane[k] + base[r];
+#pragma unroll
+                for (int p = 0; p < NPOL; ++p)
+                  if (NPOL == 1 || p < npol_used) grid_add(cell + (size_t)p * plane_sz, comp, lo_off, cmul(sv[r][p], c[r][k]));
+              }
+            }
+          }
+        }
+      }
+      return;
     }
     int run_base = -1;
     float2 acc[SLOTS][NPOL];
@@ -294,7 +356,7 @@ __device__ __forceinline__ void scatter_q(const GridRecord<NPOL> &rec, const ddf
 // box -- plain loads and stores, no atomics: within one record every lane owns different cells,
 // and a __syncwarp orders one record's updates before the next's -- and then adds every touched
 // tile cell to the grid once.  The grid sees one addition per touched cell instead of one per tap
-// (S^2 per record), which also makes the compensated additions cheap.
+// (S^2 per record).
 // Pitch 39 = 7 (mod 16): with 8-byte cells a 128-byte shared-memory wavefront holds 16 cells, and
 // the rows of a 7 x 7 footprint (lanes 0-6 row 0, 7-13 row 1, ...) then fall on distinct banks.
 constexpr int kTileW = 32, kTileH = 32, kTilePitch = 39;
@@ -379,47 +441,12 @@ __device__ __forceinline__ bool scatter_tile(const GridRecord<1> &rec, const ddf
   }
   // one grid addition per touched tile cell (cells no tap reached hold an exact zero)
   float2 *gbase = (float2 *)f.grid + ((size_t)(g0 * f.npol) * f.ny + y0) * f.nx + x0;
-  const bool comp = f.grid_lo != nullptr;
-  const ptrdiff_t lo_off = comp ? (float2 *)f.grid_lo - (float2 *)f.grid : 0;
-  if (comp) {
-    // four cells per lane at a time, so four returning atomics are in flight before their TwoSums
-    for (int i0 = lane; i0 < ncell; i0 += 128) {
-      float2 v[4], a[4];
-      float2 *cell[4];
-#pragma unroll
-      for (int k = 0; k < 4; ++k) {
-        const int i = i0 + 32 * k;
-        v[k] = czero();
-        cell[k] = gbase;
-        if (i < ncell) {
-          const int r = (int)(((unsigned)i * inv_bw) >> 16), c = i - r * bw;
-          v[k] = tile[r * kTilePitch + c];
-          cell[k] = gbase + (size_t)r * f.nx + c;
-        }
-      }
-#pragma unroll
-      for (int k = 0; k < 4; ++k) {
-        a[k] = czero();
-        if (v[k].x != 0.f || v[k].y != 0.f)
-          asm volatile("atom.global.v2.f32.add {%0, %1}, [%2], {%3, %4};"
-                       : "=f"(a[k].x), "=f"(a[k].y)
-                       : "l"(cell[k]), "f"(v[k].x), "f"(v[k].y)
-                       : "memory");
-      }
-#pragma unroll
-      for (int k = 0; k < 4; ++k) {
-        if (v[k].x != 0.f || v[k].y != 0.f) {
-          const float2 e = two_sum_err(a[k], v[k]);
-          if (e.x != 0.f || e.y != 0.f) red_add(cell[k] + lo_off, e);
-        }
-      }
-    }
-  } else {
-    for (int i = lane; i < ncell; i += 32) {
-      const int r = (int)(((unsigned)i * inv_bw) >> 16), c = i - r * bw;
-      const float2 v = tile[r * kTilePitch + c];
-      if (v.x != 0.f || v.y != 0.f) red_add(gbase + (size_t)r * f.nx + c, v);
-    }
+  const bool comp = f.grid_acc != nullptr;
+  const ptrdiff_t acc_off = acc_offset(f);
+  for (int i = lane; i < ncell; i += 32) {
+    const int r = (int)(((unsigned)i * inv_bw) >> 16), c = i - r * bw;
+    const float2 v = tile[r * kTilePitch + c];
+    if (v.x != 0.f || v.y != 0.f) grid_add(gbase + (size_t)r * f.nx + c, comp, acc_off, v);
   }
   __syncwarp();
   return true;

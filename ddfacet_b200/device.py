@@ -272,14 +272,16 @@ class FacetGrid:
     sumwt: Optional[torch.Tensor] = None        # float64 [nband, npol]
     sumjones: Optional[torch.Tensor] = None     # float64 [2, nband]
     sumjones_chan: Optional[torch.Tensor] = None  # float64 [2, nchan]
-    grid_lo: Optional[torch.Tensor] = None      # complex64 like grid: compensated gridding (all zero)
+    grid_acc: Optional[torch.Tensor] = None     # complex128 like grid: FP64 accumulation (all zero)
 
-    def with_compensation(self) -> "FacetGrid":
-        """This facet with a compensation buffer (ddfg_facet.grid_lo): gridding into it adds the
-        float32 rounding error of every grid addition to the buffer and folds it into the grid at
-        the end of each call, so each call adds the correctly rounded sum of its contributions."""
-        if self.grid_lo is None:
-            self.grid_lo = torch.zeros_like(self.grid)
+    def with_fp64_accumulation(self) -> "FacetGrid":
+        """This facet with an FP64 accumulator (ddfg_facet.grid_acc): gridding adds every tap
+        product into it with FP64 atomics and, at the end of each call, adds it into the float32
+        grid (one rounding per cell) and zeroes it, so each call adds the correctly rounded sum of
+        its contributions.  Costs as much as float32 accumulation on B200 (the atomics do not
+        return a value) and twice the grid's memory."""
+        if self.grid_acc is None:
+            self.grid_acc = torch.zeros(self.grid.shape, dtype=torch.complex128, device=self.grid.device)
         return self
 
     def struct(self, degrid=False) -> _abi.Facet:
@@ -300,7 +302,7 @@ class FacetGrid:
         s.sumwt = _ptr(self.sumwt)
         s.sumjones = _ptr(self.sumjones)
         s.sumjones_chan = _ptr(self.sumjones_chan)
-        s.grid_lo = None if degrid else _ptr(self.grid_lo)
+        s.grid_acc = None if degrid else _ptr(self.grid_acc)
         return s
 
 
@@ -363,14 +365,17 @@ def make_pol(corr_ids, stokes_ids) -> _abi.Pol:
 class Batch:
     """Scheduling of the batched (persistent, queue-driven) calls and their workspace
     (ddfg_batch): facets per pack, stripes per queue item, resident CTAs per SM (0 = library
-    default); ``static`` replaces the queue by a fixed item order (for measurements) and ``tiles``
-    has the gridder's warps sum each stripe in a shared-memory tile before adding it to the grid."""
+    default); ``static`` replaces the queue by a fixed item order (for measurements), ``tiles``
+    has the gridder's warps sum each stripe in a shared-memory tile before adding it to the grid,
+    and ``spread`` interleaves the items over one contiguous region of the block order per CTA
+    (concurrent CTAs work on distant parts of a uv-ordered map)."""
     workspace: torch.Tensor
     facets_per_pack: int = 0
     stripes_per_item: int = 0
     ctas_per_sm: int = 0
     static: bool = False
     tiles: bool = False
+    spread: bool = False
 
     @classmethod
     def create(cls, device=None, **kw) -> "Batch":
@@ -385,12 +390,13 @@ class Batch:
         b.facets_per_pack = int(self.facets_per_pack)
         b.stripes_per_item = int(self.stripes_per_item)
         b.ctas_per_sm = int(self.ctas_per_sm)
-        b.flags = (1 if self.static else 0) | (2 if self.tiles else 0)
+        b.flags = (1 if self.static else 0) | (2 if self.tiles else 0) | (4 if self.spread else 0)
         return b
 
     def describe(self) -> dict:
         return {"facets_per_pack": int(self.facets_per_pack), "stripes_per_item": int(self.stripes_per_item),
-                "ctas_per_sm": int(self.ctas_per_sm), "queue": not self.static, "tiles": bool(self.tiles)}
+                "ctas_per_sm": int(self.ctas_per_sm), "queue": not self.static, "tiles": bool(self.tiles),
+                "spread": bool(self.spread)}
 
 
 def grid(vs: VisData, facets: List[FacetGrid], pol: _abi.Pol, jones: Optional[JonesData] = None, dopsf=False,

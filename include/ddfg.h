@@ -69,14 +69,14 @@ typedef struct ddfg_facet {
   double *sumwt;               /* [nband][npol]   (sumwt)                                 */
   double *sumjones;            /* [2][nband]      (LJones[17])                            */
   double *sumjones_chan;       /* [2][nchan]      (LJones[18])                            */
-  /* Compensated gridding (optional; NULL = plain float32 accumulation).  A complex64 buffer of
-   * the grid's shape, all zero on entry, that ddfg_grid / ddfg_grid_batched use for the rounding
-   * error of every grid addition (TwoSum of the value an atomic add returns and the addend); at the
-   * end of the call it is added into grid once and left all zero again.  The grid then holds the
-   * float32 rounding of the call's exact sum (plus its previous contents) instead of the sum of
-   * ~10^4-10^6 successively rounded additions per cell.  No counterpart in the reference, which adds
-   * its double products into the float grid (gridder.h:360-362). */
-  void *grid_lo;
+  /* FP64 accumulation (optional; NULL = float32 atomic additions into grid).  A complex128 buffer
+   * [nband][npol][ny][nx], all zero on entry: ddfg_grid / ddfg_grid_batched add every tap product
+   * into it with FP64 atomics instead of into grid, and at the end of the call add it into grid
+   * (one float32 rounding per cell: grid = fl(grid + acc)) and zero it again.  The grid then holds
+   * the float32 rounding of the call's sum instead of the sum of ~10^4-10^6 successively rounded
+   * float32 additions per cell, as the reference's FP64 products would give if its grid were
+   * wider (gridder.h:360-362 adds them into the float grid one by one). */
+  void *grid_acc;
 } ddfg_facet;
 
 /* The visibilities and everything indexed by row/channel (facet independent). */
@@ -156,7 +156,10 @@ typedef struct ddfg_batch {
   int32_t flags;               /* bit 0: static item order instead of the queue (for
                                   measurements); bit 1: the gridder's warps sum each stripe into a
                                   shared-memory tile and add the touched cells to the grid once
-                                  (one Stokes plane; pays when a stripe's footprints overlap) */
+                                  (one Stokes plane; pays when a stripe's footprints overlap);
+                                  bit 2: spread the items over as many contiguous regions of the
+                                  block order as the launch has CTAs, taken in turn (CTAs work far
+                                  apart: for maps in uv-cell order, on distant grid cells) */
 } ddfg_batch;
 
 /* Library and device checks. */

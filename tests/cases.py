@@ -164,22 +164,22 @@ def _gpu_objs(c, model_grid=None, vis=None):
     return vs, fg, jd
 
 
-def run_gpu_grid(c, dopsf=False, batched=False, compensated=False, batch_kw=None):
+def run_gpu_grid(c, dopsf=False, batched=False, fp64_acc=False, batch_kw=None):
     """GPU grid of case c through ddfg_grid, or ddfg_grid_batched (``batched``, with ``batch_kw``
-    for the scheduling); ``compensated`` gives the facet a compensation buffer."""
+    for the scheduling); ``fp64_acc`` gives the facet an FP64 accumulator."""
     import torch
 
     from ddfacet_b200 import device as D
 
     vs, fg, jd = _gpu_objs(c)
-    if compensated:
-        fg.with_compensation()
+    if fp64_acc:
+        fg.with_fp64_accumulation()
     batch = D.Batch.create(vs.vis.device, **(batch_kw or {})) if batched else None
     D.grid(vs, [fg], D.make_pol(c.corr_ids, c.stokes_ids), jd, dopsf=dopsf, batch=batch)
     torch.cuda.synchronize()
     out = {"grid": fg.grid.cpu().numpy(), "sumwt": fg.sumwt.cpu().numpy()}
-    if compensated:
-        out["lo_after"] = float(fg.grid_lo.abs().max().item())
+    if fp64_acc:
+        out["acc_after"] = float(fg.grid_acc.abs().max().item())
     if c.jones:
         out["sumjones"] = fg.sumjones.cpu().numpy()
         out["sumjones_chan"] = fg.sumjones_chan.cpu().numpy()

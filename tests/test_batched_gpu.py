@@ -1,14 +1,14 @@
 """The batched calls (ddfg_grid_batched / ddfg_degrid_batched: one persistent launch whose CTAs
-take work items from a queue in device memory), compensated gridding and the large-block list
-check.
+take work items from a queue in device memory), FP64-accumulated gridding and the large-block
+list check.
 
 * batched grid / degrid against the reference on single-visibility maps, averaged BDA blocks
   (modes 1 and 2), large blocks given a warp each, Jones, flags and PSF -- the same tolerances as
   tests/test_parity_gpu.py;
 * an uneven multi-facet call under several schedules (facets per pack, stripes per item, CTAs
   per SM, static order) against single-facet reference calls;
-* compensated gridding: within 1e-4 of the reference, at least as close to the FP64 restatement
-  as plain float32 accumulation, and the compensation buffer left zero;
+* FP64-accumulated gridding: within 1e-4 of the reference, at least as close to the FP64
+  restatement as float32 accumulation (below 1e-6), and the accumulator left zero;
 * ddfg_check_large_blocks rejects lists with an out-of-range, repeated, small or missing block.
 """
 import functools
@@ -111,20 +111,20 @@ def test_batched_uneven_facets(batch_kw):
 
 
 @pytest.mark.parametrize("batched,stokes,tiles", [(False, (1, 2), False), (True, (1, 2), False), (True, (1,), True)])
-def test_compensated_grid(batched, stokes, tiles):
+def test_fp64_accumulated_grid(batched, stokes, tiles):
     c = cases.make_case(ncorr=4, stokes_ids=stokes, nw=3, ntimes=120, nant=16, lm=(0.004, 0.002))
     f64 = cases.run_fp64_grid(c)["grid"]
     r = cases.run_ref_grid(c)["grid"]
     kw = {"tiles": True} if tiles else None
     plain = cases.run_gpu_grid(c, batched=batched, batch_kw=kw)
-    comp = cases.run_gpu_grid(c, batched=batched, compensated=True, batch_kw=kw)
+    comp = cases.run_gpu_grid(c, batched=batched, fp64_acc=True, batch_kw=kw)
     e_plain, e_comp = cases.rel_rms(plain["grid"], f64), cases.rel_rms(comp["grid"], f64)
-    print(f"rel RMS vs FP64: plain {e_plain:.2e}, compensated {e_comp:.2e}, reference {cases.rel_rms(r, f64):.2e}")
+    print(f"rel RMS vs FP64: float32 sums {e_plain:.2e}, FP64 sums {e_comp:.2e}, reference {cases.rel_rms(r, f64):.2e}")
     assert cases.rel_rms(comp["grid"], r) < TOL
     np.testing.assert_array_equal(comp["grid"] != 0, r != 0)
     np.testing.assert_allclose(comp["sumwt"], plain["sumwt"], rtol=1e-12)
     assert e_comp <= e_plain * 1.01 and e_comp < 1e-6
-    assert comp["lo_after"] == 0.0
+    assert comp["acc_after"] == 0.0
 
 
 def test_large_block_check_rejects_bad_lists():
@@ -151,3 +151,39 @@ def test_large_block_check_rejects_bad_lists():
             replace(vs, large_blocks=lst.contiguous()).check_large_blocks()
         assert ei.value.code == _abi.DDFG_EMAP, why
     vs.check_large_blocks()
+
+
+@pytest.mark.parametrize("name", ["single", "bda1_jones"])
+def test_autotune_sample_is_a_strided_subset(name):
+    """The autotuner's sample: whole stripes at an even stride, each sampled block's record equal to
+    the original block's, and the sample grids like the same blocks in the full map."""
+    import torch
+
+    from ddfacet_b200 import autotune, device as D
+
+    c = _case(name)
+    vs = cases._gpu_objs(c)[0]
+    sv = autotune.sample_blocks(vs, vs.nblocks // 4)
+    nstripes, want = (vs.nblocks + 31) // 32, (vs.nblocks // 4 + 31) // 32
+    stripes = [s * nstripes // want for s in range(want)]
+    order = [s * 32 + k for s in stripes for k in range(32) if s * 32 + k < vs.nblocks]
+    assert sv.nblocks == len(order)
+    m, bs = vs.bda_map.cpu().numpy(), vs.block_start.cpu().numpy()
+    sm, sbs = sv.bda_map.cpu().numpy(), sv.block_start.cpu().numpy()
+    for i, b in enumerate(order):
+        n = m[2 + b]
+        assert sm[2 + i] == n
+        np.testing.assert_array_equal(sm[sbs[i]:sbs[i] + n], m[bs[b]:bs[b] + n])
+    # gridding the sample equals gridding the full map with the other blocks sparsified away
+    keep = torch.zeros(vs.nblocks, dtype=torch.bool, device=vs.vis.device)
+    keep[torch.tensor(order, device=vs.vis.device)] = True
+    from dataclasses import replace
+    pol = D.make_pol(c.corr_ids, c.stokes_ids)
+    objs = cases._gpu_objs(c)
+    g_full = objs[1]
+    D.grid(replace(vs, sparsification=keep.to(torch.uint8)), [g_full], pol, objs[2])
+    objs2 = cases._gpu_objs(c)
+    g_s = objs2[1]
+    D.grid(sv, [g_s], pol, objs2[2])
+    torch.cuda.synchronize()
+    assert cases.rel_rms(g_s.grid.cpu().numpy(), g_full.grid.cpu().numpy()) < 1e-6

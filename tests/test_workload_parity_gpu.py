@@ -5,15 +5,15 @@ calls the benchmark makes.
 
 * grids of corner, edge and centre facets against the reference's own gridder on those facets
   (<= 1e-4 relative RMS, identical touched cells, weight sums to 1e-9) and against the FP64
-  restatement (compensated gridding: <= 1e-5 relative RMS; the plain float32 error is printed
-  beside it);
+  restatement (FP64-accumulated gridding: <= 1e-5 relative RMS);
 * the summed prediction of the same facets (one batched degrid call into zeros) against the sum of
   the reference's per-facet predictions (<= 1e-4);
 * every block's integer footprint -- w-plane, CF table (conjugate or not), centre cell,
   oversampling offsets, sub-kernel -- word for word against the FP64 restatement of
   gridder.h:321-351 / degridder.h:168-200, for the gridder's and the degridder's block means;
 * at a quarter of the track (58 M visibilities, ~2e4 grid additions per cell on average) the
-  compensated grid of two facets against the FP64 restatement over all rows.
+  FP64-accumulated grid of two facets against the FP64 restatement over all rows, beside float32
+  accumulation.
 """
 import numpy as np
 import pytest
@@ -82,7 +82,7 @@ def test_workload_grid_against_reference_and_fp64(small):
     for f in w.facets_grid:
         f.grid.zero_()
         f.sumwt.zero_()
-        f.with_compensation()
+        f.with_fp64_accumulation()
     D.grid(w.vs, w.facets_grid, w.pol, w.jones, batch=D.Batch.create(w.vs.vis.device, tiles=True))
     torch.cuda.synchronize()
     for fi in PICK:
@@ -92,15 +92,15 @@ def test_workload_grid_against_reference_and_fp64(small):
         f64 = cases.run_fp64_grid(c)
         e_ref, e64, e_ref64 = (cases.rel_rms(g, r["grid"]), cases.rel_rms(g, f64["grid"]),
                                cases.rel_rms(r["grid"], f64["grid"]))
-        print(f"facet {fi}: gpu vs reference {e_ref:.2e}; vs FP64: gpu (compensated) {e64:.2e}, "
+        print(f"facet {fi}: gpu vs reference {e_ref:.2e}; vs FP64: gpu (FP64 sums) {e64:.2e}, "
               f"reference {e_ref64:.2e}")
         assert e_ref < 1e-4
         assert e64 < 1e-5
         np.testing.assert_array_equal(g != 0, r["grid"] != 0)
         np.testing.assert_allclose(w.facets_grid[fi].sumwt.cpu().numpy(), r["sumwt"], rtol=1e-9)
-        assert float(w.facets_grid[fi].grid_lo.abs().max()) == 0.0
+        assert float(w.facets_grid[fi].grid_acc.abs().max()) == 0.0
     for f in w.facets_grid:
-        f.grid_lo = None
+        f.grid_acc = None
 
 
 def test_workload_degrid_against_reference(small):
@@ -152,9 +152,9 @@ def test_workload_integer_indices(small, degrid):
         assert np.unique(got[ok, 7]).size > 100
 
 
-def test_full_depth_compensated_vs_fp64():
+def test_full_depth_fp64_accumulation_vs_fp64():
     """A quarter of the 4-hour track (58 M visibilities x 4 correlations) gridded onto a corner and
-    the centre facet: plain float32 accumulation and compensated accumulation against FP64."""
+    the centre facet: float32 and FP64 accumulation against the FP64 restatement."""
     import torch
 
     from ddfacet_b200 import configs, device as D
@@ -167,9 +167,9 @@ def test_full_depth_compensated_vs_fp64():
         fs = [w.facets_grid[fi] for fi in pick]
         for f in fs:
             f.grid.zero_()
-            f.grid_lo = None
+            f.grid_acc = None
             if comp:
-                f.with_compensation()
+                f.with_fp64_accumulation()
         D.grid(w.vs, fs, w.pol, w.jones, batch=D.Batch.create(w.vs.vis.device, tiles=comp))
         torch.cuda.synchronize()
         errs[comp] = [fs[i].grid.cpu().numpy() for i in range(len(pick))]
@@ -177,6 +177,6 @@ def test_full_depth_compensated_vs_fp64():
         c = _case(w, fi, host["vis"], host)
         f64 = cases.run_fp64_grid(c)["grid"]
         e_plain, e_comp = cases.rel_rms(errs[False][i], f64), cases.rel_rms(errs[True][i], f64)
-        print(f"facet {fi}, {w.nvis/1e6:.0f} Mvis: rel RMS vs FP64 plain {e_plain:.2e}, compensated {e_comp:.2e}")
+        print(f"facet {fi}, {w.nvis/1e6:.0f} Mvis: rel RMS vs FP64: float32 sums {e_plain:.2e}, FP64 sums {e_comp:.2e}")
         assert e_comp < 1e-5
         assert e_comp <= e_plain * 1.01
