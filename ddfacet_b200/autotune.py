@@ -24,7 +24,7 @@ import torch
 from . import device as D
 
 GRID_CANDIDATES: List[dict] = [dict(facets_per_pack=p, stripes_per_item=s, tiles=t)
-                               for p in (4, 8, 16, 32) for s in (0, 64) for t in (False, True)]
+                               for p in (8, 16, 32) for s in (0, 64) for t in (False, True)]
 DEGRID_CANDIDATES: List[dict] = [dict(facets_per_pack=p, stripes_per_item=s) for p in (16, 32, 0) for s in (0, 64)]
 
 
@@ -48,33 +48,14 @@ def workload_key(vs: D.VisData, facets: Sequence[D.FacetGrid], pol, jones: Optio
 
 
 def sample_blocks(vs: D.VisData, nblocks: int) -> D.VisData:
-    """About ``nblocks`` blocks of ``vs`` in whole stripes (32 consecutive blocks, the kernels' unit
-    of work) taken at an even stride over the map, so the sample covers the whole uv coverage of
-    the chunk (and touches the grids the way the full call does) rather than its first rows: a
-    new packed map of those blocks, planned, with its own large-block list when ``vs`` has one."""
-    nb = int(vs.nblocks)
-    nstripes = (nb + 31) // 32
-    want = max(1, min(nstripes, (int(nblocks) + 31) // 32))
-    if want >= nstripes:
-        return vs
-    dev = vs.bda_map.device
-    stripes = torch.div(torch.arange(want, device=dev, dtype=torch.int64) * nstripes, want, rounding_mode="floor")
-    order = (stripes[:, None] * 32 + torch.arange(32, device=dev, dtype=torch.int64)[None, :]).reshape(-1)
-    order = order[order < nb]
-    sizes = vs.bda_map[2:2 + nb].to(torch.int64)[order]
-    starts = vs.block_start[order]
-    total = int(sizes.sum().item())
-    n = int(order.numel())
-    idx = torch.repeat_interleave(starts - (torch.cumsum(sizes, 0) - sizes), sizes) + torch.arange(total, device=dev)
-    m = torch.empty(2 + n + total, dtype=torch.int32, device=dev)
-    m[0], m[1] = n & 0xFFFFFFFF, n >> 32
-    m[2:2 + n] = sizes.to(torch.int32)
-    m[2 + n:] = vs.bda_map[idx]
-    block_start, single = D.VisData.plan_map(m, int(vs.vis.shape[0]), int(vs.vis.shape[1]))
-    sp = None if vs.sparsification is None else vs.sparsification[order].contiguous()
-    out = dataclasses.replace(vs, bda_map=m, block_start=block_start, nblocks=n, single_vis_blocks=single,
-                              sparsification=sp, large_blocks=None, large_min_vis=0)
-    return out.with_large_blocks(vs.large_min_vis) if vs.large_blocks is not None else out
+    """The first ``nblocks`` blocks of ``vs`` (block starts and sparsification cut; the large-block
+    list is kept, the kernels skip its entries beyond the sample).  A contiguous prefix keeps the
+    map's locality -- the CTAs of the full call work on neighbouring stripes at any moment, and
+    their L2 reuse of grid lines is what the schedules trade against each other; a sample of
+    stripes taken at a stride over the whole map loses it and ranks the schedules wrongly."""
+    n = min(int(nblocks), vs.nblocks)
+    sp = None if vs.sparsification is None else vs.sparsification[:n]
+    return dataclasses.replace(vs, block_start=vs.block_start[:n], nblocks=n, sparsification=sp)
 
 
 def _time(fn, reps: int = 2) -> float:

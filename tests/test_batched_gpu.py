@@ -152,38 +152,3 @@ def test_large_block_check_rejects_bad_lists():
         assert ei.value.code == _abi.DDFG_EMAP, why
     vs.check_large_blocks()
 
-
-@pytest.mark.parametrize("name", ["single", "bda1_jones"])
-def test_autotune_sample_is_a_strided_subset(name):
-    """The autotuner's sample: whole stripes at an even stride, each sampled block's record equal to
-    the original block's, and the sample grids like the same blocks in the full map."""
-    import torch
-
-    from ddfacet_b200 import autotune, device as D
-
-    c = _case(name)
-    vs = cases._gpu_objs(c)[0]
-    sv = autotune.sample_blocks(vs, vs.nblocks // 4)
-    nstripes, want = (vs.nblocks + 31) // 32, (vs.nblocks // 4 + 31) // 32
-    stripes = [s * nstripes // want for s in range(want)]
-    order = [s * 32 + k for s in stripes for k in range(32) if s * 32 + k < vs.nblocks]
-    assert sv.nblocks == len(order)
-    m, bs = vs.bda_map.cpu().numpy(), vs.block_start.cpu().numpy()
-    sm, sbs = sv.bda_map.cpu().numpy(), sv.block_start.cpu().numpy()
-    for i, b in enumerate(order):
-        n = m[2 + b]
-        assert sm[2 + i] == n
-        np.testing.assert_array_equal(sm[sbs[i]:sbs[i] + n], m[bs[b]:bs[b] + n])
-    # gridding the sample equals gridding the full map with the other blocks sparsified away
-    keep = torch.zeros(vs.nblocks, dtype=torch.bool, device=vs.vis.device)
-    keep[torch.tensor(order, device=vs.vis.device)] = True
-    from dataclasses import replace
-    pol = D.make_pol(c.corr_ids, c.stokes_ids)
-    objs = cases._gpu_objs(c)
-    g_full = objs[1]
-    D.grid(replace(vs, sparsification=keep.to(torch.uint8)), [g_full], pol, objs[2])
-    objs2 = cases._gpu_objs(c)
-    g_s = objs2[1]
-    D.grid(sv, [g_s], pol, objs2[2])
-    torch.cuda.synchronize()
-    assert cases.rel_rms(g_s.grid.cpu().numpy(), g_full.grid.cpu().numpy()) < 1e-6
