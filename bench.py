@@ -328,6 +328,59 @@ def fp32_peak_tflops(dev):
         torch.backends.cuda.matmul.allow_tf32 = old
 
 
+def dropin_leg(w, ndumps=32):
+    """One facet through the drop-in ClassDDEGridMachine, the way a DDFacet facet worker calls it:
+    ``put`` then ``get`` with pageable numpy arrays (copied to the device and back inside each
+    call) on the first ``ndumps`` dumps of the chunk, with its CF tables computed by the machine
+    itself (not timed).  Host wall time of the two calls; facet-visibilities per second."""
+    from ddfacet_b200 import bda
+    from ddfacet_b200.gridmachine import ClassDDEGridMachine, default_gd
+
+    obs = w.host["obs"]
+    fi = 0
+    tess = w.host["tess"]
+    fg, wt = tess.facets[fi], w.host["wterms"][fi]
+    nr = min(obs.nrow, obs.nbl * ndumps)
+    nchan = w.nchan
+    gd = default_gd()
+    gd["Image"]["Cell"] = w.info["cell_arcsec"]
+    gd["CF"]["Nw"] = len(wt.Wplanes)
+    bmap = bda.plain_map(obs.A0[:nr], obs.A1[:nr], nchan)
+    gm = ClassDDEGridMachine(gd, obs.freqs, fg.npix_facet, lmShift=(fg.l0, fg.m0), compute_cf=True, wmax=wt.wmax,
+                             bda_grid=bmap, bda_degrid=bmap, DataCorrelationFormat=[9, 10, 11, 12],
+                             ExpectedOutputStokes=[1], NFreqBands=1, Padding=1.7)
+    dirs = {"l": np.array([f.l0 for f in tess.facets]), "m": np.array([f.m0 for f in tess.facets]),
+            "I": np.ones(len(tess.facets))}
+    J = w.host["J"] if "J" in w.host else w.jones.kms.cpu().numpy()
+    tmap = w.host["tmap"] if "tmap" in w.host else w.jones.kms_tmap.cpu().numpy()
+    dico = {"DicoJones_killMS": {"Dirs": dirs, "Jones": {"Jones": np.ascontiguousarray(J, np.complex64),
+                                                          "VisToJonesChanMapping": np.zeros(nchan, np.int32)},
+                                 "TimeMapping": np.ascontiguousarray(tmap[:nr])}}
+    vis = np.ascontiguousarray(w.vs.vis[:nr].cpu().numpy())
+    uvw = np.ascontiguousarray(obs.uvw[:nr])
+    flags = np.zeros(vis.shape, bool)
+    weights = np.ones((nr, nchan), np.float32)
+    a0a1 = (np.ascontiguousarray(obs.A0[:nr]), np.ascontiguousarray(obs.A1[:nr]))
+    times = np.ascontiguousarray(obs.times[:nr])
+    chan_map = np.zeros(nchan, np.int64)
+    n = gm.GridShape[-1]
+    grid = np.zeros((1, 1, n, n), np.complex64)
+    model = np.ascontiguousarray(w.facets_model[fi].grid.cpu().numpy())
+    kw = dict(DicoJonesMatrices=dico, freqs=obs.freqs, ChanMapping=chan_map)
+    gm.put(times, uvw, vis.copy(), flags, a0a1, W=weights, ResidueGrid=grid, **kw)  # warm-up
+    gm.get(times, uvw, vis.copy(), flags, a0a1, model, ImToGrid=False, **kw)
+    t0 = time.perf_counter()
+    gm.put(times, uvw, vis, flags, a0a1, W=weights, ResidueGrid=grid, **kw)
+    t1 = time.perf_counter()
+    gm.get(times, uvw, vis, flags, a0a1, model, ImToGrid=False, **kw)
+    t2 = time.perf_counter()
+    return {"facet_Mvis_per_s": round(nr * nchan / (t2 - t0) / 1e6, 2), "put_ms": round((t1 - t0) * 1e3, 1),
+            "get_ms": round((t2 - t1) * 1e3, 1),
+            "what": (f"facet {fi}: ClassDDEGridMachine.put + get with pageable numpy arrays (a DDFacet facet "
+                     f"worker's calls), first {ndumps} dumps ({nr} rows x {nchan} ch x 4 corr, "
+                     f"{vis.nbytes / 1e6:.0f} MB of visibilities copied in and out by each call), host wall time")}
+
+
 def algorithmic(w, s2):
     """Compulsory bytes and FLOPs of one grid call and one degrid call (one pass over the chunk):
     every stream touched once.  Grid: visibilities (K complex64), flags (K bytes), weights, uvw,
@@ -623,6 +676,10 @@ def run_gpu(args):
             out["err_vs_fp64"] = err_vs_fp64(w, comp)
         except Exception as e:  # the check is reported, not allowed to drop the measurement
             out["err_vs_fp64"] = {"error": repr(e)[:300]}
+        try:
+            out["dropin"] = dropin_leg(w)
+        except Exception as e:  # reported, not allowed to drop the measurement
+            out["dropin"] = {"error": repr(e)[:300]}
         if args.workload in WORKLOADS:
             mv, cores, sample = cpu_reference(args.workload)
             out["cpu_baseline"] = {"value": round(mv, 4), "unit": UNIT, "cores": cores, "kind": "reference",

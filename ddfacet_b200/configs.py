@@ -160,7 +160,7 @@ def multifacet_dde(device=None, scale=1.0, seed=1002, nfacets_side=9, nchan=64, 
                  nfacets=len(fg))
     w.info = dict(npix=tess.npix, npix_facet=tess.npix_facet, npix_padded=npix_pad, nw=nw,
                   supports=sorted(set(int(x) for x in wts[0].Sups)), wmax=wmax, nant=64, ntimes=obs.ntimes,
-                  nbl=obs.nbl)
+                  nbl=obs.nbl, cell_arcsec=cell)
     w.host = {"obs": obs, "wterms": wts, "tess": tess, "chan_map": chan_map}
     if keep_host:
         w.host["vis"] = vis.cpu().pin_memory()
@@ -276,7 +276,7 @@ def combined_at_scale(device=None, scale=1.0, seed=1005, hour=0, nfacets_side=11
     w.info = dict(npix=tess.npix, npix_facet=tess.npix_facet, npix_padded=npix_pad, nw=nw,
                   supports=sorted(set(int(x) for x in wts[0].Sups)), wmax=wmax, nant=64, ntimes=obs.ntimes,
                   nbl=nbl, chunk=f"hour {hour} of 8: dumps {d0}-{d1 - 1} of 3600", nsrc=nsrc, ngauss=ngauss,
-                  full_track_nvis=full.nrow * nchan)
+                  full_track_nvis=full.nrow * nchan, cell_arcsec=cell)
     w.host = {"obs": obs, "wterms": wts, "tess": tess, "chan_map": chan_map, "J": J, "tmap": tmap}
     if keep_host:
         w.host["vis"] = vis.cpu().pin_memory()

@@ -6,7 +6,7 @@ list check.
   (modes 1 and 2), large blocks given a warp each, Jones, flags and PSF -- the same tolerances as
   tests/test_parity_gpu.py;
 * an uneven multi-facet call under several schedules (facets per pack, stripes per item, CTAs
-  per SM, static order) against single-facet reference calls;
+  per SM, static order, region spreading) against single-facet reference calls;
 * FP64-accumulated gridding: within 1e-4 of the reference, at least as close to the FP64
   restatement as float32 accumulation (below 1e-6), and the accumulator left zero;
 * ddfg_check_large_blocks rejects lists with an out-of-range, repeated, small or missing block.
@@ -38,7 +38,9 @@ def _case(name):
 
 @pytest.mark.parametrize("name", ["single", "bda1_jones", "bda2_blockjones", "iquv"])
 @pytest.mark.parametrize("batch_kw", [{}, {"stripes_per_item": 1, "ctas_per_sm": 1}, {"static": True},
-                                      {"tiles": True}, {"tiles": True, "stripes_per_item": 2}])
+                                      {"tiles": True}, {"tiles": True, "stripes_per_item": 2},
+                                      {"spread": True, "stripes_per_item": 1},
+                                      {"spread": True, "static": True, "stripes_per_item": 2}])
 def test_batched_against_reference(name, batch_kw):
     c = _case(name)
     r = cases.run_ref_grid(c)
@@ -80,7 +82,8 @@ def test_batched_large_block_items():
 
 @pytest.mark.parametrize("batch_kw", [{}, {"facets_per_pack": 3}, {"facets_per_pack": 1, "stripes_per_item": 3},
                                       {"facets_per_pack": 7, "static": True}, {"ctas_per_sm": 1},
-                                      {"tiles": True, "facets_per_pack": 5}])
+                                      {"tiles": True, "facets_per_pack": 5},
+                                      {"spread": True, "facets_per_pack": 4, "stripes_per_item": 1}])
 def test_batched_uneven_facets(batch_kw):
     """20 facets of four grid sizes in one batched grid and one batched degrid call, each against
     the reference on that facet alone, under several schedules."""
