@@ -213,6 +213,28 @@ __device__ __forceinline__ M2 load_m2(const float2 *J, size_t o) {
   return m;
 }
 
+// The kMS gradient's view of the forward Jones: J = K . B (JonesServer.cc:276-289), so with a
+// beam P = K0 (B0 M B1^H) K1^H and the kMS terms see M' = B0 M B1^H; the beam's own terms come
+// from give_jones exactly as the forward takes them.  In interpolation mode 1 give_jones returns
+// (sum of the coefficients)^2 times the stored matrix (its loop reads one direction once per
+// non-zero coefficient), so the kMS matrices and their gradient carry that factor (kfac).
+__device__ __forceinline__ M2 beam_sandwich(const ddfg_jones &js, int idir_beam, int tb, int cb, int a0, int a1,
+                                            const M2 &m) {
+  if (!js.beam) return m;
+  const M2 b0 = give_jones((const float2 *)js.beam, js.beam_dims, js.interp_coefs, tb, a0, idir_beam, cb,
+                           js.interp_mode);
+  const M2 b1 = give_jones((const float2 *)js.beam, js.beam_dims, js.interp_coefs, tb, a1, idir_beam, cb,
+                           js.interp_mode);
+  return m2_times(m2_times(b0, m), m2_herm(b1));
+}
+
+__device__ __forceinline__ float kms_interp_factor(const ddfg_jones &js) {
+  if (js.interp_mode != 1 || !js.interp_coefs) return 1.f;
+  float c = 0.f;
+  for (int d = 0; d < js.kms_dims[1]; ++d) c += js.interp_coefs[d];
+  return c * c;
+}
+
 __device__ __forceinline__ M2 m2_zero() {
   M2 m;
 #pragma unroll
@@ -295,6 +317,7 @@ __global__ void __launch_bounds__(256) jones_grad_kernel(const ddfg_vis vs, cons
   LaneTaps<SLOTS> lt;
   lt.reset();
   const float2 *J = (const float2 *)js.kms;
+  const float kfac = kms_interp_factor(js);
   for (int64_t s = (int64_t)blockIdx.x * nwarps + warp; s < nstripes; s += (int64_t)gridDim.x * nwarps) {
     const int64_t b = s * 32 + lane;
     DSingleIn in;
@@ -317,14 +340,16 @@ __global__ void __launch_bounds__(256) jones_grad_kernel(const ddfg_vis vs, cons
         float2 sv[4];
 #pragma unroll
         for (int p = 0; p < 4; ++p) sv[p] = (p < NPOL) ? mine[p] : czero();
-        const M2 m = corr_from_stokes(policy, sv);
+        const M2 m = beam_sandwich(js, f.idir_beam, in.jx.tb, in.jx.cb, in.jx.a0, in.jx.a1,
+                                   corr_from_stokes(policy, sv));
         o0 = kms_offset(js, in.jx.tk, f.idir_kms, in.jx.a0, in.jx.ck);
         o1 = kms_offset(js, in.jx.tk, f.idir_kms, in.jx.a1, in.jx.ck);
-        const M2 j0 = load_m2(J, o0), j1 = load_m2(J, o1);
+        const M2 j0 = m2_scale(load_m2(J, o0), make_float2(kfac, 0.f));
+        const M2 j1 = m2_scale(load_m2(J, o1), make_float2(kfac, 0.f));
         const float dec = (float)decorr_factor(vs, f, in.nu, in.irow);
         const float2 ph = cscale(phasor_turns(in.nu * (in.U * f.l0 + in.V * f.m0 + in.W * s_n0m1[fi]) * kInvC), dec);
-        const M2 q = m2_scale(m2_times(m, m2_herm(j1)), ph);  // d ph L(s) J1^H
-        const M2 r = m2_scale(m2_times(j0, m), ph);           // d ph J0 L(s)
+        const M2 q = m2_scale(m2_times(m, m2_herm(j1)), cscale(ph, kfac));  // kfac d ph M' K1^H
+        const M2 r = m2_scale(m2_times(j0, m), cscale(ph, kfac));           // kfac d ph K0 M'
         d0 = m2_times(g, m2_herm(q));
         d1 = m2_times(m2_herm(g), r);
       }
@@ -359,6 +384,7 @@ __global__ void __launch_bounds__(256) jones_grad_block_kernel(const ddfg_vis vs
   LaneTaps<SLOTS> lt;
   lt.reset();
   const float2 *J = (const float2 *)js.kms;
+  const float kfac = kms_interp_factor(js);
   for (int64_t s = (int64_t)blockIdx.x * nwarps + warp; s < nstripes; s += (int64_t)gridDim.x * nwarps) {
     const int64_t b = s * 32 + lane;
     const bool inrange = b < vs.nblocks;
@@ -405,9 +431,11 @@ __global__ void __launch_bounds__(256) jones_grad_block_kernel(const ddfg_vis vs
               o0 = p0;
               o1 = p1;
               pending = true;
-              const M2 j0 = load_m2(J, p0), j1 = load_m2(J, p1);
-              const M2 q = m2_scale(m2_times(m, m2_herm(j1)), ph);  // d ph L(s) J1^H
-              const M2 r = m2_scale(m2_times(j0, m), ph);           // d ph J0 L(s)
+              const M2 mb = beam_sandwich(js, f.idir_beam, x.tb, x.cb, x.a0, x.a1, m);
+              const M2 j0 = m2_scale(load_m2(J, p0), make_float2(kfac, 0.f));
+              const M2 j1 = m2_scale(load_m2(J, p1), make_float2(kfac, 0.f));
+              const M2 q = m2_scale(m2_times(mb, m2_herm(j1)), cscale(ph, kfac));  // kfac d ph M' K1^H
+              const M2 r = m2_scale(m2_times(j0, mb), cscale(ph, kfac));           // kfac d ph K0 M'
               d0 = m2_add(d0, m2_times(g, m2_herm(q)));
               d1 = m2_add(d1, m2_times(m2_herm(g), r));
             } else {
@@ -419,9 +447,11 @@ __global__ void __launch_bounds__(256) jones_grad_block_kernel(const ddfg_vis vs
           const JonesIdx x = jones_idx(js, mid, (d.ch0 + d.ch1) / 2);
           o0 = kms_offset(js, x.tk, f.idir_kms, x.a0, x.ck);
           o1 = kms_offset(js, x.tk, f.idir_kms, x.a1, x.ck);
-          const M2 j0 = load_m2(J, o0), j1 = load_m2(J, o1);
-          d0 = m2_times(G, m2_herm(m2_times(m, m2_herm(j1))));
-          d1 = m2_times(m2_herm(G), m2_times(j0, m));
+          const M2 mb = beam_sandwich(js, f.idir_beam, x.tb, x.cb, x.a0, x.a1, m);
+          const float2 kf = make_float2(kfac, 0.f);
+          const M2 j0 = m2_scale(load_m2(J, o0), kf), j1 = m2_scale(load_m2(J, o1), kf);
+          d0 = m2_scale(m2_times(G, m2_herm(m2_times(mb, m2_herm(j1)))), kf);
+          d1 = m2_scale(m2_times(m2_herm(G), m2_times(j0, mb)), kf);
           pending = true;
         }
       }

@@ -211,9 +211,11 @@ int ddfg_degrid_adjoint(const ddfg_vis *vs, const ddfg_jones *js, const ddfg_pol
 
 /* Backward pass of ddfg_degrid for the kMS Jones terms: with vs->vis = dLoss/dP* as above and
  * facets[i].grid the model grids of the forward pass, adds dLoss/dJ* to grad_kms (complex64,
- * the layout of js->kms, 16-byte aligned, +=).  Needs kMS Jones only, nearest direction, no amplitude/phase
- * normalisation (DDFG_EUNSUPPORTED otherwise); any BDA map, per-visibility or per-block
- * (BDAJones) Jones.  No counterpart in the reference. */
+ * the layout of js->kms, 16-byte aligned, +=).  kMS Jones alone or times a beam (the beam is a
+ * constant: J = K.B, so the kMS terms see B0 M B1^H), nearest or weighted directions
+ * (interpolation mode 1 scales the stored matrices by the squared sum of the coefficients, as
+ * the forward does); no amplitude/phase normalisation or amplitude scaling (DDFG_EUNSUPPORTED);
+ * any BDA map, per-visibility or per-block (BDAJones) Jones.  No counterpart in the reference. */
 int ddfg_degrid_jones_grad(const ddfg_vis *vs, const ddfg_jones *js, const ddfg_pol *pol,
                            const ddfg_facet *facets, int nfacets, void *grad_kms, void *stream);
 

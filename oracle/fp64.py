@@ -178,7 +178,7 @@ def block_indices(uvw, flags, freqs, chan_map, bda_map, wplanes, wconj, overs, r
 
 
 def predict_np(bda_map, uvw, freqs, chan_map, a0, a1, facets, kms=None, kms_tmap=None, kms_cmap=None,
-               only=None):
+               only=None, beam=None, beam_tmap=None, beam_cmap=None, coefs=None):
     """Per-facet FP64 predictions P_f (complex128 [nrow][nchan][4]) of the differentiable prediction
     P = sum_f J0 (s_f I) J1^H exp(+2 pi i nu (u l0 + v m0 + w (n0 - 1)) / c), s_f the degridder's tap
     sum sum CF G_f at each block's footprint (Stokes I from four linear correlations, XX = YY = I;
@@ -186,7 +186,10 @@ def predict_np(bda_map, uvw, freqs, chan_map, a0, a1, facets, kms=None, kms_tmap
     float64 with complex128 grids and Jones -- so finite differences can take steps float32 cannot
     hold.  The integer footprints come from block_indices (the FP64 restatement of
     degridder.h:138-200).  facets: dicts with grid (complex [1][1][N][N]), wplanes, wconj, overs,
-    ref_wave, wmax, incr, cu, cv, l0, m0, idir.  ``only``: indices of the facets to evaluate."""
+    ref_wave, wmax, incr, cu, cv, l0, m0, idir (and idir_beam with a beam).  ``only``: indices of
+    the facets to evaluate.  With ``beam`` each antenna's Jones is J = K B (JonesServer.cc:276-289);
+    with interpolation ``coefs`` (mode 1) every matrix is scaled by (sum of coefs)^2, which is what
+    the reference's GiveJones loop (JonesServer.cc:71-93) returns for the facet's direction."""
     bm = np.ascontiguousarray(bda_map, np.int32)
     nb = int(np.uint32(bm[0])) + (int(bm[1]) << 32)
     sizes = bm[2:2 + nb].astype(np.int64)
@@ -234,10 +237,16 @@ def predict_np(bda_map, uvw, freqs, chan_map, a0, a1, facets, kms=None, kms_tmap
         ph = np.exp(2j * np.pi * k_nu[vc] * (u[:, 0] * f["l0"] + u[:, 1] * f["m0"] + u[:, 2] * n0m1))
         P = np.zeros((nrow, nchan, 4), np.complex128)
         if kms is not None:
+            kf = 1.0 if coefs is None else float(np.sum(np.asarray(coefs, np.float64))) ** 2
             J = np.asarray(kms, np.complex128)
             t, ch = np.asarray(kms_tmap)[vr], np.asarray(kms_cmap)[vc]
-            J0 = J[t, f["idir"], np.asarray(a0)[vr], ch].reshape(-1, 2, 2)
-            J1 = J[t, f["idir"], np.asarray(a1)[vr], ch].reshape(-1, 2, 2)
+            J0 = kf * J[t, f["idir"], np.asarray(a0)[vr], ch].reshape(-1, 2, 2)
+            J1 = kf * J[t, f["idir"], np.asarray(a1)[vr], ch].reshape(-1, 2, 2)
+            if beam is not None:
+                B = np.asarray(beam, np.complex128)
+                tb, cb, db = np.asarray(beam_tmap)[vr], np.asarray(beam_cmap)[vc], f.get("idir_beam", 0)
+                J0 = J0 @ (kf * B[tb, db, np.asarray(a0)[vr], cb].reshape(-1, 2, 2))
+                J1 = J1 @ (kf * B[tb, db, np.asarray(a1)[vr], cb].reshape(-1, 2, 2))
             M = np.einsum("nij,nkj->nik", J0, np.conj(J1))             # J0 J1^H
         else:
             M = np.broadcast_to(np.eye(2, dtype=np.complex128), (vr.size, 2, 2))

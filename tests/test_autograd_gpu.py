@@ -32,7 +32,7 @@ LMS = [(0.004, -0.002), (-0.006, 0.005)]
 MAPS = {"single": {}, "bda": dict(bda_mode=1, dphi=np.sqrt(6 * 0.05))}
 
 
-def _setup(jones=True, kind="single", jones_mode=1):
+def _setup(jones=True, kind="single", jones_mode=1, beam=False, interp_mode=0):
     cs = [cases.make_case(seed=17, nant=8, ntimes=12, nchan=8, ncorr=4, stokes_ids=(1,), nw=3, lm=lm, **MAPS[kind])
           for lm in LMS]
     for c in cs[1:]:
@@ -42,7 +42,7 @@ def _setup(jones=True, kind="single", jones_mode=1):
         assert cs[0].nrow * cs[0].nchan / nb > 1.5  # the blocks do average
     if jones:
         for i, c in enumerate(cs):
-            cases.add_jones(c, mode=jones_mode, nt=3, nd=3, idir=i + 1)
+            cases.add_jones(c, mode=jones_mode, nt=3, nd=3, idir=i + 1, beam=beam, interp_mode=interp_mode)
     objs = [cases._gpu_objs(c) for c in cs]
     setup = PredictSetup(vs=objs[0][0], facets=[o[1] for o in objs], pol=D.make_pol(cs[0].corr_ids, [1]),
                          jones=objs[0][2])
@@ -97,17 +97,19 @@ def test_dot_product_adjoint(kind, jones_mode, npairs):
 def _np_facets(cs, grids):
     return [dict(grid=g.astype(np.complex128), wplanes=c.wt.Wplanes, wconj=c.wt.WplanesConj, overs=int(c.winfos[3]),
                  ref_wave=c.wt.RefWave, wmax=c.wt.wmax, incr=c.incr, cu=c.wt.Cu, cv=c.wt.Cv, l0=c.lm[0], m0=c.lm[1],
-                 idir=c.jones["idir_kms"]) for c, g in zip(cs, grids)]
+                 idir=c.jones["idir_kms"], idir_beam=c.jones["idir_beam"]) for c, g in zip(cs, grids)]
 
 
-def _fd_check(bda, uvw, freqs, chan_map, a0, a1, facets, kms, tmap, cmap, V, w, g_grids, g_kms, rng, ncoord, h=1e-6):
+def _fd_check(bda, uvw, freqs, chan_map, a0, a1, facets, kms, tmap, cmap, V, w, g_grids, g_kms, rng, ncoord, h=1e-6,
+              **extra):
     """Central differences of L = 1/2 sum w |V - sum_f P_f|^2 at h (float64 steps on complex128
     grids and Jones) at ncoord random coordinates, half Jones and half model grid, against the GPU
-    gradient: norm-wise relative differences (Jones, grids)."""
+    gradient: norm-wise relative differences (Jones, grids).  ``extra``: beam / interpolation
+    arguments of oracle/fp64.py predict_np."""
     from oracle import fp64
 
     kms = np.asarray(kms, np.complex128)
-    Ps = fp64.predict_np(bda, uvw, freqs, chan_map, a0, a1, facets, kms, tmap, cmap)
+    Ps = fp64.predict_np(bda, uvw, freqs, chan_map, a0, a1, facets, kms, tmap, cmap, **extra)
     total = sum(Ps)
     wv = np.asarray(w, np.float64)[:, :, None]
     Vd = np.asarray(V, np.complex128)
@@ -135,7 +137,7 @@ def _fd_check(bda, uvw, freqs, chan_map, a0, a1, facets, kms, tmap, cmap, V, w, 
             for sgn in (1, -1):
                 k2 = kms.copy()
                 k2[idx] += sgn * step
-                Pn.append(fp64.predict_np(bda, uvw, freqs, chan_map, a0, a1, facets, k2, tmap, cmap, only=aff))
+                Pn.append(fp64.predict_np(bda, uvw, freqs, chan_map, a0, a1, facets, k2, tmap, cmap, only=aff, **extra))
             dl = dloss(aff, Pn[0], Pn[1])
             g = g_kms[idx]
         else:
@@ -148,7 +150,7 @@ def _fd_check(bda, uvw, freqs, chan_map, a0, a1, facets, kms, tmap, cmap, V, w, 
                 gg = f2[fi]["grid"].copy()
                 gg[idx] += sgn * step
                 f2[fi]["grid"] = gg
-                Pn.append(fp64.predict_np(bda, uvw, freqs, chan_map, a0, a1, f2, kms, tmap, cmap, only=[fi]))
+                Pn.append(fp64.predict_np(bda, uvw, freqs, chan_map, a0, a1, f2, kms, tmap, cmap, only=[fi], **extra))
             dl = dloss([fi], Pn[0], Pn[1])
             g = g_grids[fi][idx]
         fd.append(dl / (2 * h))
@@ -174,6 +176,31 @@ def test_finite_differences_h1e6(kind):
     ej, eg = _fd_check(cs[0].bda, cs[0].uvw, cs[0].freqs, cs[0].chan_map, j["A0"], j["A1"], _np_facets(cs, grids), kms,
                        j["kms_tmap"], j["kms_cmap"], V, w, gg, gk, rng, 64)
     print(f"central differences h=1e-6 (FP64, {kind}) vs GPU gradient: Jones {ej:.2e}  grid {eg:.2e}")
+    assert ej < 1e-5 and eg < 1e-5
+
+
+@pytest.mark.parametrize("kind,beam,interp", [("single", True, 0), ("bda", True, 0), ("single", False, 1),
+                                               ("bda", True, 1)])
+def test_jones_gradient_beam_and_weighted_directions(kind, beam, interp):
+    """The kMS Jones gradient with a beam (J = K B, the beam held constant) and with weighted
+    directions (interpolation mode 1): central differences h = 1e-6 in FP64 (oracle/fp64.py
+    predict_np with the beam and the interpolation factor) at 32 coordinates, norm-wise <= 1e-5."""
+    cs, setup = _setup(jones=True, kind=kind, jones_mode=1, beam=beam, interp_mode=interp)
+    rng = np.random.default_rng(19)
+    grids = [g.cpu().numpy() * np.float32(0.01) for g in _rand_grids(setup, rng)]
+    kms = np.ascontiguousarray(cs[0].jones["kms"], np.complex64)
+    V, w = cs[0].vis, cs[0].weights
+    gg, gk, _ = _gpu_loss_grads(setup, grids, kms, V, w)
+    j = cs[0].jones
+    extra = {}
+    if beam:
+        extra.update(beam=j["beam"], beam_tmap=j["beam_tmap"], beam_cmap=j["beam_cmap"])
+    if interp:
+        extra.update(coefs=j["coefs"])
+    ej, eg = _fd_check(cs[0].bda, cs[0].uvw, cs[0].freqs, cs[0].chan_map, j["A0"], j["A1"], _np_facets(cs, grids), kms,
+                       j["kms_tmap"], j["kms_cmap"], V, w, gg, gk, rng, 32, **extra)
+    print(f"central differences h=1e-6 ({kind}, beam={beam}, interp mode {interp}) vs GPU gradient: "
+          f"Jones {ej:.2e}  grid {eg:.2e}")
     assert ej < 1e-5 and eg < 1e-5
 
 
@@ -302,10 +329,11 @@ def test_adjoint_matches_reference_gridder_on_residuals():
 
 
 def test_unsupported_jones_gradient_raises():
-    """The Jones gradient covers kMS Jones at the nearest direction without normalisation; weighted
-    directions are refused with the library's message (the model-grid gradient still works)."""
+    """The Jones gradient covers kMS Jones (with or without a beam, any direction weighting) without
+    normalisation; phase-only Jones are refused with the library's message (the model-grid gradient
+    still works)."""
     c = cases.make_case(seed=3, bda_mode=1, dphi=np.sqrt(6 * 0.05), nchan=8, ncorr=4)
-    cases.add_jones(c, mode=1, nt=3, nd=3, interp_mode=1)
+    cases.add_jones(c, mode=1, nt=3, nd=3, apply_amp=0)
     vs, fg, jd = cases._gpu_objs(c)
     setup = PredictSetup(vs=vs, facets=[fg], pol=D.make_pol(c.corr_ids, c.stokes_ids), jones=jd)
     x = torch.zeros_like(fg.grid).requires_grad_(True)
@@ -313,7 +341,7 @@ def test_unsupported_jones_gradient_raises():
     assert gx.shape == x.shape
     k = jd.kms.clone().requires_grad_(True)
     P = predict(setup, [x.detach()], k)
-    with pytest.raises(ValueError, match="nearest direction"):
+    with pytest.raises(ValueError, match="normalisation"):
         torch.autograd.grad(P.real.sum(), [k])
 
 
