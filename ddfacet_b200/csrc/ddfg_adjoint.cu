@@ -235,6 +235,43 @@ __device__ __forceinline__ float kms_interp_factor(const ddfg_jones &js) {
   return c * c;
 }
 
+// The kMS matrix the forward applies, from the stored one: the interpolation factor, then the
+// amplitude / phase normalisation of norm_jones (amplitude scaling is not differentiated here).
+__device__ __forceinline__ M2 kms_forward(const M2 &z, const ddfg_jones &js) {
+  M2 k = z;
+  norm_jones(k, js, 0., 0.);
+  return k;
+}
+
+// dL/dz* of one Jones element z whose forward value is f(z) = norm_jones(z), given G = dL/df*:
+// the Wirtinger chain rule dL/dz* = conj(G) df/dz* + G conj(df/dz).  Phase only (f = z/|z|):
+// G/(2|z|) - conj(G) z^2/(2|z|^3); amplitude only (f = |z|): Re(G) z/|z|; both (f = 1): 0.  At
+// z = 0 the forward leaves a phase-only element unchanged (gradient G) and gives |z| = 0 for an
+// amplitude-only one (gradient taken as 0).
+__device__ __forceinline__ float2 norm_grad1(float2 z, float2 G, bool amp, bool phase) {
+  if (amp && phase) return G;
+  const float r = cabs2(z);
+  if (!amp && !phase) return czero();
+  if (r == 0.f) return amp ? czero() : G;
+  if (!amp) {
+    const float2 z2 = cmul(z, z);
+    const float2 t = cmul(cconj(G), z2);
+    const float inv2r = 0.5f / r, inv2r3 = 0.5f / (r * r * r);
+    return make_float2(G.x * inv2r - t.x * inv2r3, G.y * inv2r - t.y * inv2r3);
+  }
+  return cscale(z, G.x / r);
+}
+
+// dL/d(stored kMS matrix)* from dL/dK*: the normalisation's chain rule, then the interpolation
+// factor (the stored matrix z_s enters as z = kfac z_s).
+__device__ __forceinline__ M2 kms_chain(const M2 &dK, const M2 &z, const ddfg_jones &js, float kfac) {
+  M2 out;
+  const bool amp = js.apply_amp != 0, phase = js.apply_phase != 0;
+#pragma unroll
+  for (int p = 0; p < 4; ++p) out.v[p] = cscale(norm_grad1(z.v[p], dK.v[p], amp, phase), kfac);
+  return out;
+}
+
 __device__ __forceinline__ M2 m2_zero() {
   M2 m;
 #pragma unroll
@@ -344,14 +381,15 @@ __global__ void __launch_bounds__(256) jones_grad_kernel(const ddfg_vis vs, cons
                                    corr_from_stokes(policy, sv));
         o0 = kms_offset(js, in.jx.tk, f.idir_kms, in.jx.a0, in.jx.ck);
         o1 = kms_offset(js, in.jx.tk, f.idir_kms, in.jx.a1, in.jx.ck);
-        const M2 j0 = m2_scale(load_m2(J, o0), make_float2(kfac, 0.f));
-        const M2 j1 = m2_scale(load_m2(J, o1), make_float2(kfac, 0.f));
+        const M2 z0 = m2_scale(load_m2(J, o0), make_float2(kfac, 0.f));
+        const M2 z1 = m2_scale(load_m2(J, o1), make_float2(kfac, 0.f));
+        const M2 j0 = kms_forward(z0, js), j1 = kms_forward(z1, js);
         const float dec = (float)decorr_factor(vs, f, in.nu, in.irow);
         const float2 ph = cscale(phasor_turns(in.nu * (in.U * f.l0 + in.V * f.m0 + in.W * s_n0m1[fi]) * kInvC), dec);
-        const M2 q = m2_scale(m2_times(m, m2_herm(j1)), cscale(ph, kfac));  // kfac d ph M' K1^H
-        const M2 r = m2_scale(m2_times(j0, m), cscale(ph, kfac));           // kfac d ph K0 M'
-        d0 = m2_times(g, m2_herm(q));
-        d1 = m2_times(m2_herm(g), r);
+        const M2 q = m2_scale(m2_times(m, m2_herm(j1)), ph);  // d ph M' K1^H
+        const M2 r = m2_scale(m2_times(j0, m), ph);           // d ph K0 M'
+        d0 = kms_chain(m2_times(g, m2_herm(q)), z0, js, kfac);
+        d1 = kms_chain(m2_times(m2_herm(g), r), z1, js, kfac);
       }
       warp_add_jones_grad(grad, valid, o0, o1, d0, d1, lane);
     }
@@ -432,12 +470,13 @@ __global__ void __launch_bounds__(256) jones_grad_block_kernel(const ddfg_vis vs
               o1 = p1;
               pending = true;
               const M2 mb = beam_sandwich(js, f.idir_beam, x.tb, x.cb, x.a0, x.a1, m);
-              const M2 j0 = m2_scale(load_m2(J, p0), make_float2(kfac, 0.f));
-              const M2 j1 = m2_scale(load_m2(J, p1), make_float2(kfac, 0.f));
-              const M2 q = m2_scale(m2_times(mb, m2_herm(j1)), cscale(ph, kfac));  // kfac d ph M' K1^H
-              const M2 r = m2_scale(m2_times(j0, mb), cscale(ph, kfac));           // kfac d ph K0 M'
-              d0 = m2_add(d0, m2_times(g, m2_herm(q)));
-              d1 = m2_add(d1, m2_times(m2_herm(g), r));
+              const M2 z0 = m2_scale(load_m2(J, p0), make_float2(kfac, 0.f));
+              const M2 z1 = m2_scale(load_m2(J, p1), make_float2(kfac, 0.f));
+              const M2 j0 = kms_forward(z0, js), j1 = kms_forward(z1, js);
+              const M2 q = m2_scale(m2_times(mb, m2_herm(j1)), ph);  // d ph M' K1^H
+              const M2 r = m2_scale(m2_times(j0, mb), ph);           // d ph K0 M'
+              d0 = m2_add(d0, kms_chain(m2_times(g, m2_herm(q)), z0, js, kfac));
+              d1 = m2_add(d1, kms_chain(m2_times(m2_herm(g), r), z1, js, kfac));
             } else {
               G = m2_add(G, m2_scale(g, cconj(ph)));
             }
@@ -449,9 +488,10 @@ __global__ void __launch_bounds__(256) jones_grad_block_kernel(const ddfg_vis vs
           o1 = kms_offset(js, x.tk, f.idir_kms, x.a1, x.ck);
           const M2 mb = beam_sandwich(js, f.idir_beam, x.tb, x.cb, x.a0, x.a1, m);
           const float2 kf = make_float2(kfac, 0.f);
-          const M2 j0 = m2_scale(load_m2(J, o0), kf), j1 = m2_scale(load_m2(J, o1), kf);
-          d0 = m2_scale(m2_times(G, m2_herm(m2_times(mb, m2_herm(j1)))), kf);
-          d1 = m2_scale(m2_times(m2_herm(G), m2_times(j0, mb)), kf);
+          const M2 z0 = m2_scale(load_m2(J, o0), kf), z1 = m2_scale(load_m2(J, o1), kf);
+          const M2 j0 = kms_forward(z0, js), j1 = kms_forward(z1, js);
+          d0 = kms_chain(m2_times(G, m2_herm(m2_times(mb, m2_herm(j1)))), z0, js, kfac);
+          d1 = kms_chain(m2_times(m2_herm(G), m2_times(j0, mb)), z1, js, kfac);
           pending = true;
         }
       }

@@ -178,7 +178,7 @@ def block_indices(uvw, flags, freqs, chan_map, bda_map, wplanes, wconj, overs, r
 
 
 def predict_np(bda_map, uvw, freqs, chan_map, a0, a1, facets, kms=None, kms_tmap=None, kms_cmap=None,
-               only=None, beam=None, beam_tmap=None, beam_cmap=None, coefs=None):
+               only=None, beam=None, beam_tmap=None, beam_cmap=None, coefs=None, apply_amp=True, apply_phase=True):
     """Per-facet FP64 predictions P_f (complex128 [nrow][nchan][4]) of the differentiable prediction
     P = sum_f J0 (s_f I) J1^H exp(+2 pi i nu (u l0 + v m0 + w (n0 - 1)) / c), s_f the degridder's tap
     sum sum CF G_f at each block's footprint (Stokes I from four linear correlations, XX = YY = I;
@@ -189,7 +189,9 @@ def predict_np(bda_map, uvw, freqs, chan_map, a0, a1, facets, kms=None, kms_tmap
     ref_wave, wmax, incr, cu, cv, l0, m0, idir (and idir_beam with a beam).  ``only``: indices of
     the facets to evaluate.  With ``beam`` each antenna's Jones is J = K B (JonesServer.cc:276-289);
     with interpolation ``coefs`` (mode 1) every matrix is scaled by (sum of coefs)^2, which is what
-    the reference's GiveJones loop (JonesServer.cc:71-93) returns for the facet's direction."""
+    the reference's GiveJones loop (JonesServer.cc:71-93) returns for the facet's direction; without
+    ``apply_amp`` / ``apply_phase`` the kMS elements are normalised as NormJones does
+    (JonesServer.cc:25-52): z / |z| (phase only), |z| (amplitude only)."""
     bm = np.ascontiguousarray(bda_map, np.int32)
     nb = int(np.uint32(bm[0])) + (int(bm[1]) << 32)
     sizes = bm[2:2 + nb].astype(np.int64)
@@ -242,6 +244,12 @@ def predict_np(bda_map, uvw, freqs, chan_map, a0, a1, facets, kms=None, kms_tmap
             t, ch = np.asarray(kms_tmap)[vr], np.asarray(kms_cmap)[vc]
             J0 = kf * J[t, f["idir"], np.asarray(a0)[vr], ch].reshape(-1, 2, 2)
             J1 = kf * J[t, f["idir"], np.asarray(a1)[vr], ch].reshape(-1, 2, 2)
+            for K in (J0, J1):
+                if not apply_amp:
+                    a = np.abs(K)
+                    K[a != 0] /= a[a != 0]
+                if not apply_phase:
+                    K[...] = np.abs(K)
             if beam is not None:
                 B = np.asarray(beam, np.complex128)
                 tb, cb, db = np.asarray(beam_tmap)[vr], np.asarray(beam_cmap)[vc], f.get("idir_beam", 0)

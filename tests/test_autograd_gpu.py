@@ -32,7 +32,7 @@ LMS = [(0.004, -0.002), (-0.006, 0.005)]
 MAPS = {"single": {}, "bda": dict(bda_mode=1, dphi=np.sqrt(6 * 0.05))}
 
 
-def _setup(jones=True, kind="single", jones_mode=1, beam=False, interp_mode=0):
+def _setup(jones=True, kind="single", jones_mode=1, beam=False, interp_mode=0, apply_amp=1, apply_phase=1):
     cs = [cases.make_case(seed=17, nant=8, ntimes=12, nchan=8, ncorr=4, stokes_ids=(1,), nw=3, lm=lm, **MAPS[kind])
           for lm in LMS]
     for c in cs[1:]:
@@ -42,7 +42,8 @@ def _setup(jones=True, kind="single", jones_mode=1, beam=False, interp_mode=0):
         assert cs[0].nrow * cs[0].nchan / nb > 1.5  # the blocks do average
     if jones:
         for i, c in enumerate(cs):
-            cases.add_jones(c, mode=jones_mode, nt=3, nd=3, idir=i + 1, beam=beam, interp_mode=interp_mode)
+            cases.add_jones(c, mode=jones_mode, nt=3, nd=3, idir=i + 1, beam=beam, interp_mode=interp_mode,
+                            apply_amp=apply_amp, apply_phase=apply_phase)
     objs = [cases._gpu_objs(c) for c in cs]
     setup = PredictSetup(vs=objs[0][0], facets=[o[1] for o in objs], pol=D.make_pol(cs[0].corr_ids, [1]),
                          jones=objs[0][2])
@@ -179,13 +180,17 @@ def test_finite_differences_h1e6(kind):
     assert ej < 1e-5 and eg < 1e-5
 
 
-@pytest.mark.parametrize("kind,beam,interp", [("single", True, 0), ("bda", True, 0), ("single", False, 1),
-                                               ("bda", True, 1)])
-def test_jones_gradient_beam_and_weighted_directions(kind, beam, interp):
-    """The kMS Jones gradient with a beam (J = K B, the beam held constant) and with weighted
-    directions (interpolation mode 1): central differences h = 1e-6 in FP64 (oracle/fp64.py
-    predict_np with the beam and the interpolation factor) at 32 coordinates, norm-wise <= 1e-5."""
-    cs, setup = _setup(jones=True, kind=kind, jones_mode=1, beam=beam, interp_mode=interp)
+@pytest.mark.parametrize("kind,beam,interp,amp,phase", [("single", True, 0, 1, 1), ("bda", True, 0, 1, 1),
+                                                         ("single", False, 1, 1, 1), ("bda", True, 1, 1, 1),
+                                                         ("single", False, 0, 0, 1), ("bda", True, 0, 0, 1),
+                                                         ("single", False, 0, 1, 0)])
+def test_jones_gradient_beam_weighted_normalised(kind, beam, interp, amp, phase):
+    """The kMS Jones gradient with a beam (J = K B, the beam held constant), with weighted directions
+    (interpolation mode 1) and through the phase-only / amplitude-only normalisation: central
+    differences h = 1e-6 in FP64 (oracle/fp64.py predict_np with the same Jones model) at 32
+    coordinates, norm-wise <= 1e-5."""
+    cs, setup = _setup(jones=True, kind=kind, jones_mode=1, beam=beam, interp_mode=interp, apply_amp=amp,
+                       apply_phase=phase)
     rng = np.random.default_rng(19)
     grids = [g.cpu().numpy() * np.float32(0.01) for g in _rand_grids(setup, rng)]
     kms = np.ascontiguousarray(cs[0].jones["kms"], np.complex64)
@@ -197,9 +202,11 @@ def test_jones_gradient_beam_and_weighted_directions(kind, beam, interp):
         extra.update(beam=j["beam"], beam_tmap=j["beam_tmap"], beam_cmap=j["beam_cmap"])
     if interp:
         extra.update(coefs=j["coefs"])
+    extra.update(apply_amp=bool(amp), apply_phase=bool(phase))
     ej, eg = _fd_check(cs[0].bda, cs[0].uvw, cs[0].freqs, cs[0].chan_map, j["A0"], j["A1"], _np_facets(cs, grids), kms,
                        j["kms_tmap"], j["kms_cmap"], V, w, gg, gk, rng, 32, **extra)
-    print(f"central differences h=1e-6 ({kind}, beam={beam}, interp mode {interp}) vs GPU gradient: "
+    print(f"central differences h=1e-6 ({kind}, beam={beam}, interp mode {interp}, amp={amp}, phase={phase}) "
+          f"vs GPU gradient: "
           f"Jones {ej:.2e}  grid {eg:.2e}")
     assert ej < 1e-5 and eg < 1e-5
 
@@ -329,11 +336,11 @@ def test_adjoint_matches_reference_gridder_on_residuals():
 
 
 def test_unsupported_jones_gradient_raises():
-    """The Jones gradient covers kMS Jones (with or without a beam, any direction weighting) without
-    normalisation; phase-only Jones are refused with the library's message (the model-grid gradient
-    still works)."""
+    """The Jones gradient covers kMS Jones with or without a beam, any direction weighting and the
+    amplitude / phase normalisation; amplitude scaling (ScaleAmp) is refused with the library's
+    message (the model-grid gradient still works)."""
     c = cases.make_case(seed=3, bda_mode=1, dphi=np.sqrt(6 * 0.05), nchan=8, ncorr=4)
-    cases.add_jones(c, mode=1, nt=3, nd=3, apply_amp=0)
+    cases.add_jones(c, mode=1, nt=3, nd=3, scale=1, calib_err=10.0)
     vs, fg, jd = cases._gpu_objs(c)
     setup = PredictSetup(vs=vs, facets=[fg], pol=D.make_pol(c.corr_ids, c.stokes_ids), jones=jd)
     x = torch.zeros_like(fg.grid).requires_grad_(True)
@@ -341,7 +348,7 @@ def test_unsupported_jones_gradient_raises():
     assert gx.shape == x.shape
     k = jd.kms.clone().requires_grad_(True)
     P = predict(setup, [x.detach()], k)
-    with pytest.raises(ValueError, match="normalisation"):
+    with pytest.raises(ValueError, match="amplitude scaling"):
         torch.autograd.grad(P.real.sum(), [k])
 
 
