@@ -9,12 +9,14 @@ The hot path shards without a data-path collective in the two ways the facet mac
   same visibilities.  Gridding needs no exchange; the degridded predictions of all ranks are
   summed once per chunk (``reduce_predictions``), which the reference does by serialising the
   subtraction of every facet process into one shared array (degridder.h:236-263).
+  ``sharded_residual_step`` composes the two for one chunk.
 
 Everything here runs on CPU tensors with the gloo backend as well (tested that way).
 """
 from __future__ import annotations
 
-from typing import List
+import dataclasses
+from typing import Callable, List, Optional, Sequence
 
 import torch
 import torch.distributed as dist
@@ -46,3 +48,27 @@ def max_over_ranks(value: float, device=None, group=None) -> float:
         dist.all_reduce(t, op=dist.ReduceOp.MAX, group=group)
         return float(t.item())
     return float(value)
+
+
+def sharded_residual_step(vs, facets_model: Sequence, facets_grid: Sequence, pol, jones, rank: int, world: int,
+                          group=None, batch_degrid=None, batch_grid=None, degrid: Optional[Callable] = None,
+                          grid: Optional[Callable] = None) -> List[int]:
+    """One major-cycle pass over a chunk with the facets sharded over ``world`` ranks that share the
+    chunk's visibilities: this rank degrids its facets into a zero buffer (the library's degridder
+    subtracts, so the buffer holds minus its facets' prediction), the buffers are summed over ranks
+    (``reduce_predictions``), the sum is added to ``vs.vis`` (every rank then holds the same
+    residual visibilities) and this rank grids the residuals onto its facets.  Returns the indices
+    of this rank's facets.  ``degrid`` / ``grid`` default to the library's batched calls
+    (``device.degrid`` / ``device.grid``)."""
+    if degrid is None or grid is None:
+        from . import device as D
+
+        degrid = degrid or D.degrid
+        grid = grid or D.grid
+    mine = shard_facets(len(facets_model), rank, world)
+    pred = torch.zeros_like(vs.vis)
+    degrid(dataclasses.replace(vs, vis=pred), [facets_model[i] for i in mine], pol, jones, batch=batch_degrid)
+    reduce_predictions(pred, group=group)
+    vs.vis.add_(pred)
+    grid(vs, [facets_grid[i] for i in mine], pol, jones, batch=batch_grid)
+    return mine

@@ -63,3 +63,81 @@ def test_facet_sharding_and_prediction_reduction_gloo():
 def test_shard_facets_covers_all(n, w):
     got = [parallel.shard_facets(n, r, w) for r in range(w)]
     assert sorted(sum(got, [])) == list(range(n))
+
+
+# ---- the composed sharded step, with stand-in degrid / grid calls (CPU tensors) ----
+
+import dataclasses  # noqa: E402
+
+
+@dataclasses.dataclass
+class _Vis:
+    vis: torch.Tensor
+
+
+@dataclasses.dataclass
+class _Facet:
+    value: complex
+    acc: torch.Tensor
+
+
+def _fake_degrid(vs, facets, pol, jones, batch=None):
+    """Subtracts each facet's "prediction" value * (1 + row index) from every visibility."""
+    ramp = torch.arange(vs.vis.shape[0], dtype=torch.float32)[:, None] + 1
+    for f in facets:
+        vs.vis -= f.value * ramp
+
+
+def _fake_grid(vs, facets, pol, jones, batch=None):
+    """Adds the residuals, weighted by the facet's value, to each facet's accumulator."""
+    for f in facets:
+        f.acc += (vs.vis * f.value).sum(dim=0)
+
+
+def _problem(nf=7):
+    vis = torch.complex(torch.arange(40.0).reshape(10, 4), torch.ones(10, 4))
+    model = [_Facet(complex(f + 1, -f), torch.zeros(4, dtype=torch.complex64)) for f in range(nf)]
+    gridf = [_Facet(complex(1, f), torch.zeros(4, dtype=torch.complex64)) for f in range(nf)]
+    return _Vis(vis.to(torch.complex64)), model, gridf
+
+
+def _step_worker(rank, world, port, q):
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    import datetime
+
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        vs, model, gridf = _problem()
+        mine = parallel.sharded_residual_step(vs, model, gridf, None, None, rank, world, degrid=_fake_degrid,
+                                              grid=_fake_grid)
+        q.put((rank, mine, vs.vis.numpy().tolist(), [gridf[i].acc.numpy().tolist() for i in mine]))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_sharded_residual_step_gloo():
+    """Two ranks sharing a chunk: both end with the residuals of all facets' predictions, and each
+    facet is gridded exactly once, with the same result as one rank doing every facet."""
+    import numpy as np
+
+    world = 2
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_step_worker, args=(r, world, port, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    out = sorted([q.get(timeout=120) for _ in range(world)])
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    vs, model, gridf = _problem()
+    mine = parallel.sharded_residual_step(vs, model, gridf, None, None, 0, 1, degrid=_fake_degrid, grid=_fake_grid)
+    assert mine == list(range(len(model)))
+    for o in out:
+        np.testing.assert_allclose(np.array(o[2]), vs.vis.numpy(), rtol=1e-6)
+    got = {f: acc for o in out for f, acc in zip(o[1], o[3])}
+    assert sorted(got) == list(range(len(model)))
+    for f, acc in got.items():
+        np.testing.assert_allclose(np.array(acc), gridf[f].acc.numpy(), rtol=1e-5)
