@@ -117,7 +117,10 @@ def tune(vs: D.VisData, facets_grid: Sequence[D.FacetGrid], facets_model: Sequen
                for f in facets_grid]
     table: Dict[str, list] = {"grid": [], "degrid": []}
     best_g, best_gms = None, float("inf")
-    for cand in (grid_candidates or GRID_CANDIDATES):
+    cands = list(grid_candidates or GRID_CANDIDATES)
+    if not vs.single_vis_blocks:  # warp tiles serve single-visibility maps only; the library ignores them otherwise
+        cands = [c for c in cands if not c.get("tiles")]
+    for cand in cands:
         b = D.Batch.create(dev, **cand)
         ms = _time(lambda: D.grid(sv, scratch, pol, jones, batch=b))
         table["grid"].append((cand, round(ms, 3)))
