@@ -18,9 +18,8 @@ Gradients follow PyTorch's complex convention (for a real loss, ``z.grad`` is
 dLoss/dRe z + i dLoss/dIm z).  Phases, smearing factors and Jones products are recomputed in the
 backward kernels from the same inputs rather than stored.  Supported: every BDA map (blocks of
 one visibility or averaged, per-visibility or per-block Jones); for the Jones gradient, kMS Jones
-alone or times a beam (the beam is held constant), nearest or weighted directions, through the
-amplitude / phase normalisation, not through amplitude scaling (the library returns
-DDFG_EUNSUPPORTED for it).
+alone or times a beam (the beam is held constant), nearest or weighted directions, through every
+normalisation of the reference's Jones server (amplitude, phase, amplitude scaling).
 """
 from __future__ import annotations
 

@@ -366,8 +366,7 @@ extern "C" int ddfg_degrid_jones_grad(const ddfg_vis *vs, const ddfg_jones *js, 
   int policy = -1;
   int rc = degrid_checks(vs, js, pol, facets, nfacets, &policy);
   if (rc) return rc;
-  if (js->mode == 0 || !js->kms || js->scale_jones)
-    return ddfg_set_error(DDFG_EUNSUPPORTED, "degrid_jones_grad: needs kMS Jones without amplitude scaling");
+  if (js->mode == 0 || !js->kms) return ddfg_set_error(DDFG_EUNSUPPORTED, "degrid_jones_grad: needs kMS Jones");
   if (!grad_kms) return ddfg_set_error(DDFG_EINVAL, "degrid_jones_grad: null gradient array");
   if ((uintptr_t)grad_kms & 15)
     return ddfg_set_error(DDFG_EINVAL, "degrid_jones_grad: the gradient array must be 16-byte aligned");

@@ -235,40 +235,69 @@ __device__ __forceinline__ float kms_interp_factor(const ddfg_jones &js) {
   return c * c;
 }
 
-// The kMS matrix the forward applies, from the stored one: the interpolation factor, then the
-// amplitude / phase normalisation of norm_jones (amplitude scaling is not differentiated here).
-__device__ __forceinline__ M2 kms_forward(const M2 &z, const ddfg_jones &js) {
+// The kMS matrix the forward applies, from the interpolated one z: the normalisation of
+// norm_jones at the uv the forward uses (amplitude scaling depends on it).
+__device__ __forceinline__ M2 kms_forward(const M2 &z, const ddfg_jones &js, double u, double v) {
   M2 k = z;
-  norm_jones(k, js, 0., 0.);
+  norm_jones(k, js, u, v);
   return k;
 }
 
-// dL/dz* of one Jones element z whose forward value is f(z) = norm_jones(z), given G = dL/df*:
-// the Wirtinger chain rule dL/dz* = conj(G) df/dz* + G conj(df/dz).  Phase only (f = z/|z|):
-// G/(2|z|) - conj(G) z^2/(2|z|^3); amplitude only (f = |z|): Re(G) z/|z|; both (f = 1): 0.  At
-// z = 0 the forward leaves a phase-only element unchanged (gradient G) and gives |z| = 0 for an
-// amplitude-only one (gradient taken as 0).
-__device__ __forceinline__ float2 norm_grad1(float2 z, float2 G, bool amp, bool phase) {
-  if (amp && phase) return G;
+// dL/dz* for f = z/|z|, given G = dL/df* (the Wirtinger chain rule dL/dz* = conj(G) df/dz* +
+// G conj(df/dz)): G/(2|z|) - conj(G) z^2/(2|z|^3); at z = 0 the forward leaves z unchanged.
+__device__ __forceinline__ float2 unit_grad(float2 z, float2 G) {
   const float r = cabs2(z);
-  if (!amp && !phase) return czero();
-  if (r == 0.f) return amp ? czero() : G;
-  if (!amp) {
-    const float2 z2 = cmul(z, z);
-    const float2 t = cmul(cconj(G), z2);
-    const float inv2r = 0.5f / r, inv2r3 = 0.5f / (r * r * r);
-    return make_float2(G.x * inv2r - t.x * inv2r3, G.y * inv2r - t.y * inv2r3);
-  }
-  return cscale(z, G.x / r);
+  if (r == 0.f) return G;
+  const float2 t = cmul(cconj(G), cmul(z, z));
+  const float inv2r = 0.5f / r, inv2r3 = 0.5f / (r * r * r);
+  return make_float2(G.x * inv2r - t.x * inv2r3, G.y * inv2r - t.y * inv2r3);
 }
 
-// dL/d(stored kMS matrix)* from dL/dK*: the normalisation's chain rule, then the interpolation
-// factor (the stored matrix z_s enters as z = kfac z_s).
-__device__ __forceinline__ M2 kms_chain(const M2 &dK, const M2 &z, const ddfg_jones &js, float kfac) {
+// dL/dz* of one Jones element through norm_jones (JonesServer.cc:25-52), given G = dL/df* for its
+// output: the forward applies z1 = amplitude normalisation (z/|z|, without ApplyAmp), z2 = phase
+// removal (|z1|, without ApplyPhase), z3 = amplitude scaling z2 ((1 - alpha)/|z2| + alpha)
+// (DoScaleJones), and the chain rule runs back through the three: scaling gives
+// (1 - alpha) unit_grad + alpha G, phase removal Re(G) z1/|z1|, amplitude normalisation unit_grad.
+__device__ __forceinline__ float2 norm_grad1(float2 z, float2 G, bool amp, bool phase, bool scale, float alpha) {
+  float2 z1 = z;
+  if (!amp) {
+    const float a = cabs2(z);
+    if (a != 0.f) z1 = cscale(z, 1.f / a);
+  }
+  const float2 z2 = phase ? z1 : make_float2(cabs2(z1), 0.f);
+  float2 g = G;
+  if (scale) {
+    const float2 u = unit_grad(z2, g);
+    g = cabs2(z2) == 0.f ? g : make_float2((1.f - alpha) * u.x + alpha * g.x, (1.f - alpha) * u.y + alpha * g.y);
+  }
+  if (!phase) {
+    const float r = cabs2(z1);
+    g = r == 0.f ? czero() : cscale(z1, g.x / r);
+  }
+  if (!amp) g = unit_grad(z, g);
+  return g;
+}
+
+// The amplitude-scaling factor alpha of norm_jones at (u, v).
+__device__ __forceinline__ float scale_alpha(const ddfg_jones &js, double u, double v) {
+  const double r2 = (u * u + v * v) / (js.wavelength_mean * js.wavelength_mean);
+  return (float)exp(-2. * kPi * js.calib_error * js.calib_error * r2);
+}
+
+// dL/d(stored kMS matrix)* from dL/dK*: the normalisation's chain rule at (u, v), then the
+// interpolation factor (the stored matrix z_s enters as z = kfac z_s).
+__device__ __forceinline__ M2 kms_chain(const M2 &dK, const M2 &z, const ddfg_jones &js, float kfac, double u,
+                                        double v) {
   M2 out;
-  const bool amp = js.apply_amp != 0, phase = js.apply_phase != 0;
+  const bool amp = js.apply_amp != 0, phase = js.apply_phase != 0, scale = js.scale_jones != 0;
+  if (amp && phase && !scale) {
 #pragma unroll
-  for (int p = 0; p < 4; ++p) out.v[p] = cscale(norm_grad1(z.v[p], dK.v[p], amp, phase), kfac);
+    for (int p = 0; p < 4; ++p) out.v[p] = cscale(dK.v[p], kfac);
+    return out;
+  }
+  const float alpha = scale ? scale_alpha(js, u, v) : 0.f;
+#pragma unroll
+  for (int p = 0; p < 4; ++p) out.v[p] = cscale(norm_grad1(z.v[p], dK.v[p], amp, phase, scale, alpha), kfac);
   return out;
 }
 
@@ -383,13 +412,13 @@ __global__ void __launch_bounds__(256) jones_grad_kernel(const ddfg_vis vs, cons
         o1 = kms_offset(js, in.jx.tk, f.idir_kms, in.jx.a1, in.jx.ck);
         const M2 z0 = m2_scale(load_m2(J, o0), make_float2(kfac, 0.f));
         const M2 z1 = m2_scale(load_m2(J, o1), make_float2(kfac, 0.f));
-        const M2 j0 = kms_forward(z0, js), j1 = kms_forward(z1, js);
+        const M2 j0 = kms_forward(z0, js, in.U, in.V), j1 = kms_forward(z1, js, in.U, in.V);
         const float dec = (float)decorr_factor(vs, f, in.nu, in.irow);
         const float2 ph = cscale(phasor_turns(in.nu * (in.U * f.l0 + in.V * f.m0 + in.W * s_n0m1[fi]) * kInvC), dec);
         const M2 q = m2_scale(m2_times(m, m2_herm(j1)), ph);  // d ph M' K1^H
         const M2 r = m2_scale(m2_times(j0, m), ph);           // d ph K0 M'
-        d0 = kms_chain(m2_times(g, m2_herm(q)), z0, js, kfac);
-        d1 = kms_chain(m2_times(m2_herm(g), r), z1, js, kfac);
+        d0 = kms_chain(m2_times(g, m2_herm(q)), z0, js, kfac, in.U, in.V);
+        d1 = kms_chain(m2_times(m2_herm(g), r), z1, js, kfac, in.U, in.V);
       }
       warp_add_jones_grad(grad, valid, o0, o1, d0, d1, lane);
     }
@@ -449,6 +478,7 @@ __global__ void __launch_bounds__(256) jones_grad_block_kernel(const ddfg_vis vs
         const int mid = d.rows[d.nrows / 2];
         const float dec = (float)decorr_factor(vs, f, d.freqmean, mid);
         M2 G = m2_zero();
+        double uk = 0., vk = 0.;
         for (int inx = 0; inx < d.nrows; ++inx) {
           const int64_t irow = d.rows[inx];
           const double *up = vs.uvw + 3 * irow;
@@ -460,11 +490,17 @@ __global__ void __launch_bounds__(256) jones_grad_block_kernel(const ddfg_vis vs
               const JonesIdx x = jones_idx(js, irow, ch);
               const size_t p0 = kms_offset(js, x.tk, f.idir_kms, x.a0, x.ck);
               const size_t p1 = kms_offset(js, x.tk, f.idir_kms, x.a1, x.ck);
-              if (pending && (p0 != o0 || p1 != o1)) {
-                red_add_m2(grad + o0, d0);
-                red_add_m2(grad + o1, d1);
-                d0 = m2_zero();
-                d1 = m2_zero();
+              if (!pending || p0 != o0 || p1 != o1) {
+                if (pending) {
+                  red_add_m2(grad + o0, d0);
+                  red_add_m2(grad + o1, d1);
+                  d0 = m2_zero();
+                  d1 = m2_zero();
+                }
+                // the forward's Jones cache (reset per block) recomputes the kMS terms, and reads
+                // the uv its amplitude scaling uses, at the visibility where they change
+                uk = up[0];
+                vk = up[1];
               }
               o0 = p0;
               o1 = p1;
@@ -472,11 +508,11 @@ __global__ void __launch_bounds__(256) jones_grad_block_kernel(const ddfg_vis vs
               const M2 mb = beam_sandwich(js, f.idir_beam, x.tb, x.cb, x.a0, x.a1, m);
               const M2 z0 = m2_scale(load_m2(J, p0), make_float2(kfac, 0.f));
               const M2 z1 = m2_scale(load_m2(J, p1), make_float2(kfac, 0.f));
-              const M2 j0 = kms_forward(z0, js), j1 = kms_forward(z1, js);
+              const M2 j0 = kms_forward(z0, js, uk, vk), j1 = kms_forward(z1, js, uk, vk);
               const M2 q = m2_scale(m2_times(mb, m2_herm(j1)), ph);  // d ph M' K1^H
               const M2 r = m2_scale(m2_times(j0, mb), ph);           // d ph K0 M'
-              d0 = m2_add(d0, kms_chain(m2_times(g, m2_herm(q)), z0, js, kfac));
-              d1 = m2_add(d1, kms_chain(m2_times(m2_herm(g), r), z1, js, kfac));
+              d0 = m2_add(d0, kms_chain(m2_times(g, m2_herm(q)), z0, js, kfac, uk, vk));
+              d1 = m2_add(d1, kms_chain(m2_times(m2_herm(g), r), z1, js, kfac, uk, vk));
             } else {
               G = m2_add(G, m2_scale(g, cconj(ph)));
             }
@@ -489,9 +525,10 @@ __global__ void __launch_bounds__(256) jones_grad_block_kernel(const ddfg_vis vs
           const M2 mb = beam_sandwich(js, f.idir_beam, x.tb, x.cb, x.a0, x.a1, m);
           const float2 kf = make_float2(kfac, 0.f);
           const M2 z0 = m2_scale(load_m2(J, o0), kf), z1 = m2_scale(load_m2(J, o1), kf);
-          const M2 j0 = kms_forward(z0, js), j1 = kms_forward(z1, js);
-          d0 = kms_chain(m2_times(G, m2_herm(m2_times(mb, m2_herm(j1)))), z0, js, kfac);
-          d1 = kms_chain(m2_times(m2_herm(G), m2_times(j0, mb)), z1, js, kfac);
+          const double *um = vs.uvw + 3 * (int64_t)mid;  // the forward normalises at the middle row
+          const M2 j0 = kms_forward(z0, js, um[0], um[1]), j1 = kms_forward(z1, js, um[0], um[1]);
+          d0 = kms_chain(m2_times(G, m2_herm(m2_times(mb, m2_herm(j1)))), z0, js, kfac, um[0], um[1]);
+          d1 = kms_chain(m2_times(m2_herm(G), m2_times(j0, mb)), z1, js, kfac, um[0], um[1]);
           pending = true;
         }
       }

@@ -214,9 +214,10 @@ int ddfg_degrid_adjoint(const ddfg_vis *vs, const ddfg_jones *js, const ddfg_pol
  * the layout of js->kms, 16-byte aligned, +=).  kMS Jones alone or times a beam (the beam is a
  * constant: J = K.B, so the kMS terms see B0 M B1^H), nearest or weighted directions
  * (interpolation mode 1 scales the stored matrices by the squared sum of the coefficients, as
- * the forward does), through the amplitude / phase normalisation (NormJones); not through
- * amplitude scaling (DDFG_EUNSUPPORTED); any BDA map, per-visibility or per-block (BDAJones)
- * Jones.  No counterpart in the reference. */
+ * the forward does), through NormJones (amplitude / phase normalisation and amplitude scaling,
+ * the latter at the uv the forward's Jones cache reads); needs kMS Jones (DDFG_EUNSUPPORTED
+ * otherwise); any BDA map, per-visibility or per-block (BDAJones) Jones.  No counterpart in the
+ * reference. */
 int ddfg_degrid_jones_grad(const ddfg_vis *vs, const ddfg_jones *js, const ddfg_pol *pol,
                            const ddfg_facet *facets, int nfacets, void *grad_kms, void *stream);
 

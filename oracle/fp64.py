@@ -178,7 +178,8 @@ def block_indices(uvw, flags, freqs, chan_map, bda_map, wplanes, wconj, overs, r
 
 
 def predict_np(bda_map, uvw, freqs, chan_map, a0, a1, facets, kms=None, kms_tmap=None, kms_cmap=None,
-               only=None, beam=None, beam_tmap=None, beam_cmap=None, coefs=None, apply_amp=True, apply_phase=True):
+               only=None, beam=None, beam_tmap=None, beam_cmap=None, coefs=None, apply_amp=True, apply_phase=True,
+               scale=False, calib_err=0.0, wavelength_mean=1.0):
     """Per-facet FP64 predictions P_f (complex128 [nrow][nchan][4]) of the differentiable prediction
     P = sum_f J0 (s_f I) J1^H exp(+2 pi i nu (u l0 + v m0 + w (n0 - 1)) / c), s_f the degridder's tap
     sum sum CF G_f at each block's footprint (Stokes I from four linear correlations, XX = YY = I;
@@ -191,7 +192,11 @@ def predict_np(bda_map, uvw, freqs, chan_map, a0, a1, facets, kms=None, kms_tmap
     with interpolation ``coefs`` (mode 1) every matrix is scaled by (sum of coefs)^2, which is what
     the reference's GiveJones loop (JonesServer.cc:71-93) returns for the facet's direction; without
     ``apply_amp`` / ``apply_phase`` the kMS elements are normalised as NormJones does
-    (JonesServer.cc:25-52): z / |z| (phase only), |z| (amplitude only)."""
+    (JonesServer.cc:25-52): z / |z| (phase only), |z| (amplitude only); with ``scale`` each is
+    then scaled by (1 - alpha)/|z| + alpha, alpha = exp(-2 pi calib_err^2 (u^2 + v^2) /
+    wavelength_mean^2) at the uv of the visibility where the reference's Jones cache last
+    recomputed the kMS terms (per block, rows then channels: the first visibility of each run of
+    equal time slot, antennas and Jones channel)."""
     bm = np.ascontiguousarray(bda_map, np.int32)
     nb = int(np.uint32(bm[0])) + (int(bm[1]) << 32)
     sizes = bm[2:2 + nb].astype(np.int64)
@@ -244,12 +249,24 @@ def predict_np(bda_map, uvw, freqs, chan_map, a0, a1, facets, kms=None, kms_tmap
             t, ch = np.asarray(kms_tmap)[vr], np.asarray(kms_cmap)[vc]
             J0 = kf * J[t, f["idir"], np.asarray(a0)[vr], ch].reshape(-1, 2, 2)
             J1 = kf * J[t, f["idir"], np.asarray(a1)[vr], ch].reshape(-1, 2, 2)
+            if scale:
+                key = np.stack([t, np.asarray(a0)[vr], np.asarray(a1)[vr], ch, vb], axis=1)
+                start = np.ones(vr.size, bool)
+                start[1:] = np.any(key[1:] != key[:-1], axis=1)
+                first = np.maximum.accumulate(np.where(start, np.arange(vr.size), 0))
+                uk = uvw[vr[first]]
+                r2 = (uk[:, 0] ** 2 + uk[:, 1] ** 2) / wavelength_mean ** 2
+                alpha = np.exp(-2 * np.pi * calib_err ** 2 * r2)[:, None, None]
             for K in (J0, J1):
                 if not apply_amp:
                     a = np.abs(K)
                     K[a != 0] /= a[a != 0]
                 if not apply_phase:
                     K[...] = np.abs(K)
+                if scale:
+                    a = np.abs(K)
+                    fac = np.where(a != 0, (1 - alpha) / np.where(a != 0, a, 1) + alpha, 1.0)
+                    K[...] = K * fac
             if beam is not None:
                 B = np.asarray(beam, np.complex128)
                 tb, cb, db = np.asarray(beam_tmap)[vr], np.asarray(beam_cmap)[vc], f.get("idir_beam", 0)

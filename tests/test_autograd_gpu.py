@@ -32,7 +32,8 @@ LMS = [(0.004, -0.002), (-0.006, 0.005)]
 MAPS = {"single": {}, "bda": dict(bda_mode=1, dphi=np.sqrt(6 * 0.05))}
 
 
-def _setup(jones=True, kind="single", jones_mode=1, beam=False, interp_mode=0, apply_amp=1, apply_phase=1):
+def _setup(jones=True, kind="single", jones_mode=1, beam=False, interp_mode=0, apply_amp=1, apply_phase=1, scale=0,
+           calib_err=0.0):
     cs = [cases.make_case(seed=17, nant=8, ntimes=12, nchan=8, ncorr=4, stokes_ids=(1,), nw=3, lm=lm, **MAPS[kind])
           for lm in LMS]
     for c in cs[1:]:
@@ -43,7 +44,7 @@ def _setup(jones=True, kind="single", jones_mode=1, beam=False, interp_mode=0, a
     if jones:
         for i, c in enumerate(cs):
             cases.add_jones(c, mode=jones_mode, nt=3, nd=3, idir=i + 1, beam=beam, interp_mode=interp_mode,
-                            apply_amp=apply_amp, apply_phase=apply_phase)
+                            apply_amp=apply_amp, apply_phase=apply_phase, scale=scale, calib_err=calib_err)
     objs = [cases._gpu_objs(c) for c in cs]
     setup = PredictSetup(vs=objs[0][0], facets=[o[1] for o in objs], pol=D.make_pol(cs[0].corr_ids, [1]),
                          jones=objs[0][2])
@@ -180,17 +181,19 @@ def test_finite_differences_h1e6(kind):
     assert ej < 1e-5 and eg < 1e-5
 
 
-@pytest.mark.parametrize("kind,beam,interp,amp,phase", [("single", True, 0, 1, 1), ("bda", True, 0, 1, 1),
-                                                         ("single", False, 1, 1, 1), ("bda", True, 1, 1, 1),
-                                                         ("single", False, 0, 0, 1), ("bda", True, 0, 0, 1),
-                                                         ("single", False, 0, 1, 0)])
-def test_jones_gradient_beam_weighted_normalised(kind, beam, interp, amp, phase):
+@pytest.mark.parametrize("kind,beam,interp,amp,phase,scale", [
+    ("single", True, 0, 1, 1, 0), ("bda", True, 0, 1, 1, 0), ("single", False, 1, 1, 1, 0), ("bda", True, 1, 1, 1, 0),
+    ("single", False, 0, 0, 1, 0), ("bda", True, 0, 0, 1, 0), ("single", False, 0, 1, 0, 0),
+    ("single", False, 0, 1, 1, 1), ("bda", False, 0, 1, 1, 1), ("bda", True, 0, 0, 1, 1)])
+def test_jones_gradient_beam_weighted_normalised(kind, beam, interp, amp, phase, scale):
     """The kMS Jones gradient with a beam (J = K B, the beam held constant), with weighted directions
     (interpolation mode 1) and through the phase-only / amplitude-only normalisation: central
     differences h = 1e-6 in FP64 (oracle/fp64.py predict_np with the same Jones model) at 32
     coordinates, norm-wise <= 1e-5."""
+    # a calibration error that gives alpha well inside (0, 1) at these baselines
+    ce = 0.3 * 2.998e8 / 1.375e9 / 1500.0 if scale else 0.0
     cs, setup = _setup(jones=True, kind=kind, jones_mode=1, beam=beam, interp_mode=interp, apply_amp=amp,
-                       apply_phase=phase)
+                       apply_phase=phase, scale=scale, calib_err=ce)
     rng = np.random.default_rng(19)
     grids = [g.cpu().numpy() * np.float32(0.01) for g in _rand_grids(setup, rng)]
     kms = np.ascontiguousarray(cs[0].jones["kms"], np.complex64)
@@ -203,9 +206,12 @@ def test_jones_gradient_beam_weighted_normalised(kind, beam, interp, amp, phase)
     if interp:
         extra.update(coefs=j["coefs"])
     extra.update(apply_amp=bool(amp), apply_phase=bool(phase))
+    if scale:
+        extra.update(scale=True, calib_err=ce, wavelength_mean=float(np.mean(299792458.0 / cs[0].freqs)))
     ej, eg = _fd_check(cs[0].bda, cs[0].uvw, cs[0].freqs, cs[0].chan_map, j["A0"], j["A1"], _np_facets(cs, grids), kms,
                        j["kms_tmap"], j["kms_cmap"], V, w, gg, gk, rng, 32, **extra)
-    print(f"central differences h=1e-6 ({kind}, beam={beam}, interp mode {interp}, amp={amp}, phase={phase}) "
+    print(f"central differences h=1e-6 ({kind}, beam={beam}, interp mode {interp}, amp={amp}, phase={phase}, "
+          f"scale={scale}) "
           f"vs GPU gradient: "
           f"Jones {ej:.2e}  grid {eg:.2e}")
     assert ej < 1e-5 and eg < 1e-5
@@ -335,21 +341,29 @@ def test_adjoint_matches_reference_gridder_on_residuals():
         assert e < 1e-4
 
 
-def test_unsupported_jones_gradient_raises():
-    """The Jones gradient covers kMS Jones with or without a beam, any direction weighting and the
-    amplitude / phase normalisation; amplitude scaling (ScaleAmp) is refused with the library's
-    message (the model-grid gradient still works)."""
+def test_jones_gradient_needs_kms_jones():
+    """The Jones gradient covers kMS Jones with or without a beam, any direction weighting and every
+    normalisation (amplitude, phase, amplitude scaling); with beam-only Jones the model-grid
+    gradient still works and the library refuses a Jones gradient with its message."""
+    import ctypes as C
+
+    from ddfacet_b200 import _abi
+
     c = cases.make_case(seed=3, bda_mode=1, dphi=np.sqrt(6 * 0.05), nchan=8, ncorr=4)
-    cases.add_jones(c, mode=1, nt=3, nd=3, scale=1, calib_err=10.0)
+    cases.add_jones(c, mode=1, nt=3, nd=3, kms=False, beam=True)
     vs, fg, jd = cases._gpu_objs(c)
-    setup = PredictSetup(vs=vs, facets=[fg], pol=D.make_pol(c.corr_ids, c.stokes_ids), jones=jd)
+    pol = D.make_pol(c.corr_ids, c.stokes_ids)
+    setup = PredictSetup(vs=vs, facets=[fg], pol=pol, jones=jd)
     x = torch.zeros_like(fg.grid).requires_grad_(True)
-    (gx,) = torch.autograd.grad(predict(setup, [x], jd.kms).abs().sum(), [x])
+    (gx,) = torch.autograd.grad(predict(setup, [x], None).abs().sum(), [x])
     assert gx.shape == x.shape
-    k = jd.kms.clone().requires_grad_(True)
-    P = predict(setup, [x.detach()], k)
-    with pytest.raises(ValueError, match="amplitude scaling"):
-        torch.autograd.grad(P.real.sum(), [k])
+    lib = _abi.lib()
+    arr = (_abi.Facet * 1)(fg.struct(degrid=True))
+    vss, js = vs.struct(), jd.struct()
+    grad = torch.zeros(64, dtype=torch.complex64, device=fg.grid.device)
+    rc = lib.ddfg_degrid_jones_grad(C.byref(vss), C.byref(js), C.byref(pol), arr, 1, C.c_void_p(grad.data_ptr()),
+                                    None)
+    assert rc == _abi.DDFG_EUNSUPPORTED and "kMS" in _abi.last_error()
 
 
 # ---- the model image as the leaf: image -> facet grids (crop, norm, taper, FFT) -> prediction ----
