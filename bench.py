@@ -597,9 +597,9 @@ def run_gpu(args):
     achieved = dom_bytes / (dom_ms * 1e-3) / 1e9
     # DRAM bytes (read + write) of one call of each kernel, per visibility, from the one-pass ncu
     # capture of the full chunk with the benchmark's schedules (profiles/traffic_combined_at_scale_full.md):
-    # grid 194.2 GB in one launch (FP64 accumulators), degrid 185.1 GB in eight launches of 16 facets
+    # grid 194.2 GB in one launch (FP64 accumulators), degrid 229.7 GB in eight launches of 16 facets
     # (each re-reads and rewrites the visibilities), for 232,243,200 visibilities
-    traffic_per_vis = {"grid": 194.172e9 / 232243200, "degrid": 185.078e9 / 232243200}
+    traffic_per_vis = {"grid": 194.172e9 / 232243200, "degrid": 229.674e9 / 232243200}
     K, F, G = w.ncorr, w.nfacets, w.info["npix_padded"]
     launches_grid = math.ceil(F / 128) * (2 if comp else 1)
     dpp = bd.facets_per_pack if bd.facets_per_pack > 0 else 128
